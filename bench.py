@@ -1,0 +1,306 @@
+"""Benchmark of the compact-difference hot path on B200.
+
+Workload (one "step"): the cd10 periodic first derivative, the cd10 periodic
+second derivative and the cf90 periodic filter along x, y and z -- 9 operator
+applications -- on a 512^3 FP64 field (random-phase |k|^-5/3 synthesis, seeded;
+synthetic data standing in for solver fields).  Metric: Gpts/s = output points
+of all operator applications per second (16 algorithmic bytes per point: read
+f, write df).  Inputs (1 GiB) exceed L2 (126 MB), so no flush is needed
+between iterations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU (torchrun): every rank processes its own field (lines and fields are
+independent, no data-path collective): weak scaling, value = all ranks' points
+/ max-over-ranks time.
+
+The JSON line carries: value (device-resident), e2e (the same metric through
+the host-buffer C-ABI call pado_apply_host, copies included), roofline of the
+line kernels (CUDA events, algorithmic bytes / kernel time, against the
+measured HBM copy bandwidth), cpu_baseline (the oracle -- the C restatement of
+the reference -- on the host cores), clocks sampled during the timed region,
+and the number of library kernel launches in the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 512
+OPS = [("cd10", 1), ("cd10", 2), ("cf90", 0)]  # (scheme, kind)
+METRIC = "Gpts/s cd06/cd10 dd1-3 @512^3 FP64 (%HBM peak); batched, fwd+adjoint vs plain"
+BYTES_PER_PT = 16
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic() -> float | None:
+    """DRAM bytes per launch of the line kernel from the committed ncu summary
+    (profiles/line_kernel_512cube.md, line 'traffic_bytes_per_launch: X')."""
+    p = os.path.join(ROOT, "profiles", "line_kernel_512cube.md")
+    try:
+        with open(p) as fh:
+            for line in fh:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_field(seed: int) -> np.ndarray:
+    from tests.fields import spectrum53
+
+    return spectrum53((N, N, N), seed)
+
+
+def cpu_baseline(f: np.ndarray, threads: int, budget_s: float = 20.0) -> dict:
+    """Times the oracle built with the reference's Release flags on the host cores."""
+    import oracle
+
+    dx = 2 * np.pi / N
+    ops = [oracle.OracleOp({"cd10": oracle.CD10, "cf90": oracle.CF90}[s], N, dx, True, fast=True) for s, _ in OPS]
+    out = np.empty_like(f)
+    pts = 0
+    t0 = time.perf_counter()
+    done = []
+    while time.perf_counter() - t0 < budget_s and len(done) < 9:
+        i = len(done)
+        op, (s, kind) = ops[i % 3], OPS[i % 3]
+        axis = i // 3 + 1
+        ts = time.perf_counter()
+        op.apply(kind, axis, f, N, N, 0, 0, nthreads=threads, out=out)
+        done.append(time.perf_counter() - ts)
+        pts += N ** 3
+    el = sum(done)
+    return {"value": pts / el / 1e9, "unit": "Gpts/s", "cores": threads, "kind": "port",
+            "sample": f"{len(done)} of the 9 operator applications on the 512^3 field "
+                      f"(oracle, -O3 -ffast-math -march=x86-64-v3, OpenMP {threads} threads)"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    f = make_field(7)
+    per_step = []
+    for s in range(args.warmup + args.steps):
+        cb = cpu_baseline(f, threads, budget_s=1e9 if s >= args.warmup else 30.0)
+        if s >= args.warmup:
+            per_step.append(cb["value"])
+    v = statistics.median(per_step)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gpts/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 9 * N ** 3 / (v * 1e9) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cd10 d1 + cd10 d2 + cf90, periodic, x/y/z on 512^3 FP64", "n": N,
+                       "operators_per_step": 9},
+            "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": threads, "kind": "port",
+                             "sample": "the full 9-operator step on the 512^3 field per timed step "
+                                       "(oracle = C restatement of the reference; the Fortran reference "
+                                       "cannot be built: no Fortran compiler in the image)"},
+            "e2e": {"value": v, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args) -> None:
+    import torch
+
+    import padeops_b200 as pb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    dx = 2 * np.pi / N
+    f_host = make_field(7 + rank)
+    f = torch.from_numpy(f_host).cuda()
+    df = torch.empty_like(f)
+    ops = {}
+    for s, _ in OPS:
+        op = pb.cd10() if s == "cd10" else pb.cf90()
+        assert (op.init(N, dx, True, 0, 0) if s == "cd10" else op.init(N, True)) == 0
+        ops[s] = op
+    plan = [(ops[s], kind, axis) for axis in (1, 2, 3) for s, kind in OPS]
+    stream = torch.cuda.current_stream()
+
+    def step(events=None):
+        for i, (op, kind, axis) in enumerate(plan):
+            if events is not None:
+                events[i][0].record(stream)
+            op.apply(kind, axis, f, df, N, N, 0, 0)
+            if events is not None:
+                events[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in plan]
+          for _ in range(args.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = pb.launch_count()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for k in range(args.steps):
+            step(ev[k])
+        stop.record(stream)
+        torch.cuda.synchronize()
+    launches = pb.launch_count() - launches0
+    ms = start.elapsed_time(stop)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pts = 9 * N ** 3 * args.steps * world
+    value = pts / (ms / 1e3) / 1e9
+    kern_ms = [a.elapsed_time(b) for row in ev for a, b in row]
+    per_op = {}
+    for i, (op, kind, axis) in enumerate(plan):
+        name = f"{type(op).__name__}_{'d1' if kind == 1 else ('d2' if kind == 2 else 'filter')}_axis{axis}"
+        t_op = statistics.mean(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps))
+        per_op[name] = round(N ** 3 * BYTES_PER_PT / (t_op / 1e3) / 1e9, 1)
+    avg_launch_ms = statistics.mean(kern_ms)
+    peak, peak_kind = measured_peaks()
+    achieved = N ** 3 * BYTES_PER_PT / (avg_launch_ms / 1e3) / 1e9
+
+    # end to end: host buffers through the C ABI host call, copies included
+    e2e = None
+    if rank == 0 or world > 1:
+        hf = torch.from_numpy(f_host).pin_memory()
+        hdf = torch.empty_like(hf).pin_memory()
+        e2e_steps = max(1, min(args.steps, 3))
+        for op, kind, axis in plan[:1]:
+            op.apply_host(kind, axis, hf, hdf, N, N)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for op, kind, axis in plan:
+                op.apply_host(kind, axis, hf, hdf, N, N)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        e2e = {"value": 9 * N ** 3 * e2e_steps / el / 1e9 * world, "unit": "Gpts/s",
+               "h2d_bytes_per_step": 9 * N ** 3 * 8, "d2h_bytes_per_step": 9 * N ** 3 * 8,
+               "path": "pado_apply_host per operator (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(f_host, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "cd10 d1 + cd10 d2 + cf90, periodic, x/y/z on 512^3 FP64 "
+                                       "(9 operator applications per step)",
+                           "n": N, "operators_per_step": 9, "l2": "inputs larger than L2 (1 GiB field)",
+                           "per_operator_gbs": per_op},
+                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "traffic": profiled_traffic(),
+                             "kernel": "pado::line_kernel (all 9 launches, averaged)",
+                             "peak_source": peak_kind},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pado", choices=["pado", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

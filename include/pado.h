@@ -1,0 +1,171 @@
+/*
+ * pado.h -- C ABI of padeops_b200, a B200-native (CUDA sm_100a, FP64)
+ * implementation of PadeOps' compact-difference operators.
+ *
+ * Each entry point replaces one type-bound procedure of the reference's
+ * Fortran scheme objects (paths relative to the reference project):
+ *
+ *   cd06stuff  src/derivatives/cd06.F90   init :129, dd1/dd2/dd3 :775/797/819, destroy :203
+ *   cd10stuff  src/derivatives/cd10.F90   init :195, dd1/dd2/dd3 :2029/2099/2169,
+ *                                         d2d1/d2d2/d2d3 :2239/2309/2379, destroy :317
+ *   cf90stuff  src/filters/cf90.F90       init :107, filter1/filter2/filter3 :1020/1090/1160,
+ *                                         destroy :177
+ *
+ * Conventions (the reference's):
+ *   - Fields are FP64, column-major f(n1,n2,n3): f[i + n1*(j + n2*k)].
+ *   - dd1/d2d1/filter1 act along x on an (n,na,nb) array, dd2/... along y on
+ *     (na,n,nb), dd3/... along z on (na,nb,n).
+ *   - f is intent(in) and df intent(out); they must not overlap.
+ *   - bc1/bcn select the boundary closure of a bounded (non-periodic)
+ *     operator: 0 one-sided, 1 symmetric, -1 antisymmetric.  A Fortran caller
+ *     that omits the optional arguments passes 0 (the reference's default).
+ *     cd06 ignores them (its closures are fixed at init), as do periodic
+ *     operators.
+ *   - Handles are immutable after init and may be used concurrently from
+ *     several host threads and streams.
+ *
+ * Differences from the reference, by design:
+ *   - f and df are DEVICE pointers and the work is enqueued on `stream`
+ *     (a cudaStream_t, NULL = legacy default stream); the call returns once
+ *     enqueued.  pado_apply_host() is the host-buffer variant.
+ *   - Errors are returned, never aborted on: a bad bc returns PADO_E_BC
+ *     (324, the code the reference passes to GracefulExit), init size errors
+ *     return the reference's ierr (2, 3 or 7).
+ */
+#ifndef PADO_H
+#define PADO_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pado_op_s *pado_op_t;
+
+/* schemes */
+#define PADO_CD06 0
+#define PADO_CD10 1
+#define PADO_CF90 2
+
+/* operator kinds */
+#define PADO_FILTER 0
+#define PADO_D1 1
+#define PADO_D2 2
+
+/* status codes (0 and the reference's init ierr values 2, 3, 7 are kept) */
+#define PADO_OK 0
+#define PADO_E_BC 324          /* bc1/bcn not in {0,1,-1} (cd10.F90:2044-2055)        */
+#define PADO_E_NULL (-1)       /* null handle or pointer                               */
+#define PADO_E_ALIAS (-2)      /* f and df overlap                                     */
+#define PADO_E_UNSUPPORTED (-3)/* operator the reference does not provide (cd06 d2 ...) */
+#define PADO_E_ARG (-4)        /* bad axis, kind, scheme, negative size, bad dx        */
+#define PADO_E_CUDA (-5)       /* a CUDA runtime call failed                           */
+#define PADO_E_SIZE (-6)       /* line longer than the kernels support, or overflow    */
+#define PADO_E_TIMEOUT (-7)    /* a bounded device wait expired                        */
+#define PADO_E_NOMEM (-8)      /* host or device allocation failed                     */
+#define PADO_E_STATE (-9)      /* object used in a state that does not allow the call  */
+
+/* ---- scheme objects ---------------------------------------------------- */
+
+/* cd06%init(n, dx, periodic, bc1, bcn)  -- cd06.F90:129.
+ * Returns 0, 3 (periodic, n in 2..5) or 2 (bounded, n in 2..7). */
+int pado_cd06_init(pado_op_t *op, int n, double dx, int periodic, int bc1, int bcn);
+
+/* cd10%init(n, dx, periodic, bc1, bcn)  -- cd10.F90:195.  Returns 0 or 2 (n in 2..7). */
+int pado_cd10_init(pado_op_t *op, int n, double dx, int periodic, int bc1, int bcn);
+
+/* cf90%init(n, periodic)  -- cf90.F90:107.  Returns 0 or 7 (n in 2..9). */
+int pado_cf90_init(pado_op_t *op, int n, int periodic);
+
+/* Generic form of the three inits (scheme = PADO_CD06/CD10/CF90; dx ignored by cf90). */
+int pado_create(pado_op_t *op, int scheme, int n, double dx, int periodic, int bc1, int bcn);
+
+/* %destroy  -- cd06.F90:203, cd10.F90:317, cf90.F90:177.  NULL is a no-op. */
+void pado_destroy(pado_op_t op);
+
+/* %GetSize  -- cd06.F90:123, cd10.F90:189. */
+int pado_get_size(pado_op_t op);
+
+/* ---- operators (device pointers, enqueued on `stream`) ------------------ */
+
+/* cd06%dd1/dd2/dd3 (cd06.F90:775/797/819) and cd10%dd1/dd2/dd3 (cd10.F90:2029/2099/2169). */
+int pado_dd1(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+int pado_dd2(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+int pado_dd3(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+
+/* cd10%d2d1/d2d2/d2d3 (cd10.F90:2239/2309/2379). */
+int pado_d2d1(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+int pado_d2d2(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+int pado_d2d3(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+
+/* cf90%filter1/filter2/filter3 (cf90.F90:1020/1090/1160, real variant). */
+int pado_filter1(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+int pado_filter2(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+int pado_filter3(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn, void *stream);
+
+/* Generic dispatch behind the nine calls above: kind = PADO_D1/D2/FILTER,
+ * axis = 1/2/3.  Same semantics as the reference's dd{axis}/d2d{axis}/filter{axis}. */
+int pado_apply(pado_op_t op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1, int bcn,
+               void *stream);
+
+/* Adjoint (transpose) of pado_apply: fbar = D^T g with D = A^{-1} B the
+ * operator pado_apply applies, boundary closures included.  No counterpart in
+ * the reference; used for reverse-mode differentiation. */
+int pado_apply_adjoint(pado_op_t op, int kind, int axis, const double *g, double *fbar, long na, long nb, int bc1,
+                       int bcn, void *stream);
+
+/* Host-buffer variant of pado_apply for callers whose fields live in host
+ * memory (the reference's own calling convention): copies f to the device,
+ * applies the operator and copies df back, pipelined in chunks, and returns
+ * when df holds the result.  Pinned host memory gives full overlap. */
+int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, double *df_host, long na, long nb,
+                    int bc1, int bcn, void *stream);
+
+/* ---- tuning ------------------------------------------------------------- */
+
+/* Launch shape of the line kernels for this handle: m = segment length
+ * (rows one thread solves serially, 8/16/32/64), lines = lines per CTA
+ * (8/16/32).  0 keeps the current value.  Rebuilds the handle's tables. */
+int pado_set_tiling(pado_op_t op, int m, int lines);
+int pado_get_tiling(pado_op_t op, int *m, int *lines);
+
+/* ---- batched execution (many fields, one persistent launch) ------------ */
+
+typedef struct pado_batch_s *pado_batch_t;
+
+/* One item of a batch: apply `op` (kind, axis, bc1, bcn) to field f of shape
+ * (n1,n2,n3) -- the operator's n must equal the extent along `axis` -- writing df. */
+typedef struct {
+    pado_op_t op;
+    int kind, axis, bc1, bcn;
+    long n1, n2, n3;
+    const double *f;
+    double *df;
+} pado_batch_item;
+
+int pado_batch_create(pado_batch_t *batch, const pado_batch_item *items, int nitems);
+/* Enqueue the whole batch on `stream` as one persistent kernel launch. */
+int pado_batch_run(pado_batch_t batch, void *stream);
+/* Enqueue the batch as one launch per item (the per-field loop it replaces). */
+int pado_batch_run_loop(pado_batch_t batch, void *stream);
+/* Capture pado_batch_run into a CUDA graph once and replay it on `stream`. */
+int pado_batch_run_graph(pado_batch_t batch, void *stream);
+/* Launch shape of the persistent kernel: threads per CTA (128/256/512, 0 =
+ * keep) and a cap on resident CTAs per SM (0 = as many as fit).  Used by the
+ * autotuner; drops any captured graph. */
+int pado_batch_set_config(pado_batch_t batch, int threads, int ctas_per_sm);
+/* Tiles, grid size, threads per CTA and dynamic shared memory of the batch. */
+int pado_batch_info(pado_batch_t batch, long long *ntiles, int *grid, int *threads, long long *smem_bytes);
+void pado_batch_destroy(pado_batch_t batch);
+
+/* ---- diagnostics -------------------------------------------------------- */
+
+const char *pado_strerror(int status);
+/* Number of kernel launches this process has enqueued through the library. */
+long long pado_launch_count(void);
+/* Library version string. */
+const char *pado_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PADO_H */

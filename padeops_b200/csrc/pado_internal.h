@@ -1,0 +1,61 @@
+// pado_internal.h -- definitions shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pado.h"
+#include "pado_kernels.cuh"
+#include "pado_tables.h"
+
+namespace pado {
+
+extern std::atomic<long long> g_launches;
+
+// Device-resident tables of one (kind, bc1, bcn, direction) operator.
+struct DevTables {
+    double *tab = nullptr;     // [nb][T_NF]
+    double *segsum = nullptr;  // [S][4]
+    double *bt = nullptr;      // transposed stencil blocks (adjoint, bounded)
+    double mb[4] = {0, 0, 0, 0};
+    double taps[9] = {0};
+    int nb = 0, nbord = 0;
+    Layout lay;
+    RhsCoef rc{};
+};
+
+using TabKey = std::tuple<int, int, int, int>;  // kind, bc1, bcn, adjoint
+
+int cuda_fail(cudaError_t e);
+bool kind_supported(int scheme, int kind);
+bool valid_bc(int bc);
+
+}  // namespace pado
+
+struct pado_op_s {
+    int scheme = 0, n = 0, periodic = 1, bc1 = 0, bcn = 0;
+    double dx = 1.0;
+    int m = 32, lines = 16;
+    int device = 0;
+    std::map<pado::TabKey, pado::DevTables> tables;
+    std::vector<void *> allocations;
+    // host-buffer staging
+    std::mutex staging_mu;
+    double *stage_f = nullptr, *stage_df = nullptr;
+    size_t stage_elems = 0;
+};
+
+namespace pado {
+
+// Validates an apply request and fills the launch parameters for the given
+// lines-per-CTA.  Returns PADO_OK, or an error; *trivial is set when n == 1
+// or the field is empty (nothing for a line kernel to do).
+int prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
+                   int bcn, bool adjoint, int lines, KParams *kp, bool *trivial);
+
+}  // namespace pado

@@ -1,0 +1,59 @@
+// pado_tables.h -- host-side construction of the solver tables the device
+// kernels consume: the reference's LU / Thomas / penta factorizations, their
+// conversion into the unified sweep of pado_common.h, the adjoint (transposed)
+// sweep, the segment-partition responses, and the transposed stencil blocks.
+#pragma once
+
+#include <vector>
+
+#include "pado_common.h"
+
+namespace pado {
+
+// Unified sweep coefficients for one operator (see the comment block at the
+// end of pado_common.h).  Vectors have nb entries.
+struct Sweep {
+    int n = 0, nb = 0, nbord = 0;
+    std::vector<double> alpha, c1, c2, k1, k2, gamma, d1, d2, e1, e2, delta;
+    double mb[4] = {0, 0, 0, 0};  // border map, row-major nbord x nbord
+};
+
+// Reference factorizations, column-major (n, ncol) like the Fortran arrays.
+// cd06.F90:221-262
+std::vector<double> cd06_cyclic_lu(int n, double b, double d, double a);
+// cd06.F90:264-327
+std::vector<double> cd06_tri1(int n, int bc1, int bcn);
+// cd10.F90:351-427, cf90.F90:198-274
+std::vector<double> penta_cyclic_lu(int n, double e, double a, double d, double c, double f);
+// cd10.F90:429-578 (kind D1), :580-709 (D2), cf90.F90:276-418 (filter)
+std::vector<double> penta_bounded(int scheme, int kind, int n, int bc1, int bcn);
+
+// The sweep that reproduces the reference's solve for (scheme, kind).
+// bc1/bcn: closures of a bounded line (cd06 uses its init closures).
+Sweep primal_sweep(int scheme, int kind, int n, int periodic, int bc1, int bcn);
+// The sweep of the transposed solve A^{-T}.
+Sweep adjoint_sweep(const Sweep &p);
+
+// Cut of [0, n) into S segments of length base+1 (first rem) or base.
+struct Layout {
+    int n = 0, S = 1, base = 0, rem = 0;
+    int start(int s) const { return s * base + (s < rem ? s : rem); }
+    int len(int s) const { return base + (s < rem ? 1 : 0); }
+};
+Layout make_layout(int n, int m_max);
+
+// Device table: T_NF doubles per banded row (TabField order) with the
+// segment responses folded in, plus 4 segment sums per segment
+// (k1.U, k1.V, k2.U, k2.V).
+void build_device_table(const Sweep &sw, const Layout &lay, std::vector<double> &tab, std::vector<double> &segsum);
+
+// Transposed stencil of a bounded line: B^T rows for the first and last
+// ZB columns.  Dense (n x n) when n <= DENSE_BT_MAX.
+constexpr int BT_ZONE = 8, BT_WIN = 12, DENSE_BT_MAX = 32;
+std::vector<double> transposed_stencil_blocks(const RhsCoef &rc, int n, int bc1, int bcn);
+
+// Dense B (n x n, row-major) of the explicit stencil; used by the builder
+// above and by the self-checks.
+std::vector<double> stencil_matrix(const RhsCoef &rc, int n, int bc1, int bcn);
+
+}  // namespace pado

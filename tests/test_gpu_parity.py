@@ -1,0 +1,190 @@
+"""GPU parity: every operator of the hot path, through the C ABI, against the
+oracle (the CPU restatement of the reference) on seeded inputs.
+
+Tolerance: max|x - r| / max|r| <= 1e-12 (FP64, the bar the operator set is
+held to), written per assertion below.
+"""
+import itertools
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.fields import line_len, na_nb, rel_err, sinusoids, spectrum53
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+OPS = [(oracle.CD06, oracle.D1), (oracle.CD10, oracle.D1), (oracle.CD10, oracle.D2), (oracle.CF90, oracle.FILTER)]
+BCS = list(itertools.product([0, 1, -1], [0, 1, -1]))
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _make(scheme, n, dx, periodic, bc1=0, bcn=0):
+    import padeops_b200 as pb
+
+    cls = {oracle.CD06: pb.cd06, oracle.CD10: pb.cd10, oracle.CF90: pb.cf90}[scheme]
+    op = cls()
+    ierr = op.init(n, periodic) if scheme == oracle.CF90 else op.init(n, dx, periodic, bc1, bcn)
+    assert ierr == 0
+    return op
+
+
+def _gpu_apply(torch, op, kind, axis, f, bc1, bcn, adjoint=False):
+    shape = f.shape
+    na, nb = na_nb(shape, axis)
+    ft = torch.from_numpy(np.ascontiguousarray(f)).cuda()
+    out = torch.full_like(ft, float("nan"))
+    op.apply(kind, axis, ft, out, na, nb, bc1, bcn, adjoint=adjoint)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def _oracle_apply(scheme, kind, axis, f, dx, periodic, bc1, bcn, init_bc=(0, 0)):
+    n = line_len(f.shape, axis)
+    ob1, obn = init_bc if scheme == oracle.CD06 else (0, 0)
+    o = oracle.OracleOp(scheme, n, dx, periodic, ob1, obn)
+    assert o.ierr == 0
+    na, nb = na_nb(f.shape, axis)
+    return o.apply(kind, axis, f, na, nb, bc1, bcn).reshape(f.shape)
+
+
+@pytest.mark.parametrize("scheme,kind", OPS)
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("axis", [1, 2, 3])
+def test_parity_small(torch_cuda, scheme, kind, periodic, axis):
+    torch = torch_cuda
+    shape = (19, 24, 33)  # (n3, n2, n1): odd and even line lengths
+    f = spectrum53(shape, seed=11 + axis)
+    n = line_len(shape, axis)
+    dx = 2 * np.pi / n if periodic else 1.0 / (n - 1)
+    bcs = [(0, 0)] if (periodic or scheme == oracle.CD06) else BCS
+    op = _make(scheme, n, dx, periodic)
+    for bc1, bcn in bcs:
+        got = _gpu_apply(torch, op, kind, axis, f, bc1, bcn)
+        ref = _oracle_apply(scheme, kind, axis, f, dx, periodic, bc1, bcn)
+        assert np.isfinite(got).all()
+        assert rel_err(got, ref) <= TOL, (bc1, bcn, rel_err(got, ref))
+
+
+@pytest.mark.parametrize("scheme,kind", OPS)
+@pytest.mark.parametrize("n", [8, 10, 11, 17, 32, 64, 65, 127, 256, 384, 512, 1000, 1024])
+def test_parity_line_lengths(torch_cuda, scheme, kind, n):
+    """Ragged and extreme line lengths (minimum sizes, odd, the configs' 1024)."""
+    torch = torch_cuda
+    if (scheme == oracle.CF90 and n < 10) or (scheme == oracle.CD06 and n < 8):
+        pytest.skip("below the scheme's minimum size")
+    rng = np.random.default_rng(n)
+    for axis in (1, 3):
+        shape = (3, 5, n) if axis == 1 else (n, 3, 6)
+        f = rng.standard_normal(shape)
+        for periodic in (True, False):
+            dx = 0.7
+            op = _make(scheme, n, dx, periodic)
+            for bc1, bcn in ([(0, 0)] if periodic or scheme == oracle.CD06 else [(0, 0), (1, -1), (-1, 1)]):
+                got = _gpu_apply(torch, op, kind, axis, f, bc1, bcn)
+                ref = _oracle_apply(scheme, kind, axis, f, dx, periodic, bc1, bcn)
+                assert rel_err(got, ref) <= TOL, (axis, periodic, bc1, bcn, rel_err(got, ref))
+
+
+@pytest.mark.parametrize("m,lines", [(8, 8), (8, 32), (16, 16), (32, 8), (32, 16), (64, 8)])
+def test_parity_tilings(torch_cuda, m, lines):
+    """Every segment length / lines-per-CTA the tuner may pick gives the same result."""
+    torch = torch_cuda
+    shape = (40, 16, 200)
+    f = spectrum53(shape, seed=5)
+    for scheme, kind in OPS:
+        for periodic in (True, False):
+            op = _make(scheme, 200, 0.05, periodic)
+            try:
+                op.set_tiling(m, lines)
+            except Exception:
+                continue  # not a legal shape for n = 200
+            got = _gpu_apply(torch, op, kind, 1, f, 1 if not periodic else 0, -1 if not periodic else 0)
+            ref = _oracle_apply(scheme, kind, 1, f, 0.05, periodic, 1 if not periodic else 0,
+                                -1 if not periodic else 0)
+            assert rel_err(got, ref) <= TOL
+
+
+def test_config1_cd06_64cube(torch_cuda):
+    """cd06 periodic dd1/dd2/dd3 on the 64^3 sum of 8 sinusoids (dx = 2pi/64)."""
+    torch = torch_cuda
+    n = 64
+    f = sinusoids(n, seed=1234)
+    dx = 2 * np.pi / n
+    op = _make(oracle.CD06, n, dx, True)
+    for axis in (1, 2, 3):
+        got = _gpu_apply(torch, op, oracle.D1, axis, f, 0, 0)
+        ref = _oracle_apply(oracle.CD06, oracle.D1, axis, f, dx, True, 0, 0)
+        assert rel_err(got, ref) <= TOL
+
+
+def test_cd06_bounded_init_closures(torch_cuda):
+    """cd06 bounded takes its closures from init; bc = 1 there keeps interior
+    bands (the reference's "Incomplete" branch, cd06.F90:288-291)."""
+    torch = torch_cuda
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((5, 4, 40))
+    for ib in [(0, 0), (1, 1), (0, 1), (1, 0)]:
+        op = _make(oracle.CD06, 40, 0.1, False, *ib)
+        got = _gpu_apply(torch, op, oracle.D1, 1, f, 0, 0)
+        ref = _oracle_apply(oracle.CD06, oracle.D1, 1, f, 0.1, False, 0, 0, init_bc=ib)
+        assert rel_err(got, ref) <= TOL, ib
+
+
+def test_n_equals_one(torch_cuda):
+    """n == 1: derivatives return zero, the filter returns a copy (cd10.F90:2037, cf90.F90:1028)."""
+    torch = torch_cuda
+    f = np.random.default_rng(0).standard_normal((4, 3, 1))
+    for scheme, kind in OPS:
+        op = _make(scheme, 1, 1.0, True)
+        got = _gpu_apply(torch, op, kind, 1, f, 0, 0)
+        expect = f if kind == oracle.FILTER else np.zeros_like(f)
+        assert np.array_equal(got, expect)
+
+
+def test_errors(torch_cuda):
+    import padeops_b200 as pb
+    from padeops_b200 import _lib as L
+
+    torch = torch_cuda
+    op = _make(oracle.CD10, 16, 0.1, False)
+    f = torch.zeros(16 * 4, dtype=torch.float64, device="cuda")
+    df = torch.zeros_like(f)
+    with pytest.raises(pb.PadoError) as e:
+        op.dd1(f, df, 2, 2, 2, 0)
+    assert e.value.status == L.E_BC == 324
+    with pytest.raises(pb.PadoError) as e:
+        op.dd1(f, f, 2, 2)
+    assert e.value.status == L.E_ALIAS
+    c6 = _make(oracle.CD06, 16, 0.1, True)
+    with pytest.raises(pb.PadoError) as e:
+        c6.apply(L.D2, 1, f, df, 2, 2)
+    assert e.value.status == L.E_UNSUPPORTED
+    with pytest.raises(ValueError):
+        op.dd1(f.cpu(), df, 2, 2)  # no CPU path
+    assert pb.cd06().init(5, 0.1, True, 0, 0) == 3
+    assert pb.cd06().init(7, 0.1, False, 0, 0) == 2
+    assert pb.cd10().init(7, 0.1, True, 0, 0) == 2
+    assert pb.cf90().init(9, True) == 7
+
+
+def test_launch_count_and_library(torch_cuda):
+    """The CUDA library is what runs: launches are counted by the extension."""
+    import padeops_b200 as pb
+
+    torch = torch_cuda
+    before = pb.launch_count()
+    op = _make(oracle.CD10, 32, 0.1, True)
+    f = torch.randn(32 * 9, dtype=torch.float64, device="cuda")
+    df = torch.empty_like(f)
+    op.dd2(f, df, 3, 3)
+    torch.cuda.synchronize()
+    assert pb.launch_count() == before + 1
