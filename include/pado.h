@@ -127,6 +127,12 @@ int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, doub
  * (8/16/32).  0 keeps the current value.  Rebuilds the handle's tables. */
 int pado_set_tiling(pado_op_t op, int m, int lines);
 int pado_get_tiling(pado_op_t op, int *m, int *lines);
+/* Kernel organisation of the forward operator: 1 = one CTA per tile of
+ * lines (the default, 0 selects it), 2 = persistent CTAs that prefetch the
+ * next tile with cp.async while the current one is solved, 3 = persistent
+ * CTAs that read lines straight into registers and warm L2 with the next
+ * tile (strided axes; x lines use 2). */
+int pado_set_kernel_variant(pado_op_t op, int variant);
 
 /* ---- batched execution (many fields, one persistent launch) ------------ */
 

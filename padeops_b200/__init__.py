@@ -3,7 +3,9 @@
 A drop-in for the hot path of PadeOps: the cd06 / cd10 Pade derivatives and
 the cf90 compact filter along x, y and z, periodic or bounded, behind the C
 ABI of include/pado.h (for the Fortran solver) and the reference-shaped
-Python objects below.  The CUDA library is required; there is no CPU path.
+Python objects below.  The CUDA library (padeops_b200/_lib/libpado.so) is
+required: the first operation loads it and raises ImportError if it is
+missing.  There is no CPU path.
 """
 from . import _lib
 from ._lib import CD06, CD10, CF90, D1, D2, FILTER, PadoError
@@ -11,9 +13,6 @@ from .operators import Derivatives, Filters, cd06, cd10, cf90
 
 __all__ = ["cd06", "cd10", "cf90", "Derivatives", "Filters", "PadoError", "CD06", "CD10", "CF90", "D1", "D2",
            "FILTER", "launch_count", "version"]
-
-_lib.lib()  # load now: fail loudly if the extension was not built
-
 
 def launch_count() -> int:
     """Kernel launches this process has enqueued through the library."""

@@ -13,6 +13,8 @@
 
 #include "pado_internal.h"
 
+#include <algorithm>
+
 using namespace pado;
 
 namespace pado {
@@ -40,6 +42,8 @@ bool kind_supported(int scheme, int kind)
 
 namespace {
 
+int max_threads_for_m(int m) { return m >= 64 ? 256 : 512; }
+
 int upload(pado_op_s *op, const std::vector<double> &h, double **d)
 {
     if (h.empty()) {
@@ -59,15 +63,11 @@ int upload(pado_op_s *op, const std::vector<double> &h, double **d)
 // Default tiling: segment length and lines per CTA for a line of length n.
 void default_tiling(int n, int *m, int *lines)
 {
-    *m = n >= 192 ? 32 : (n > 64 ? 16 : (n > 32 ? 16 : 8));
-    if (n > 32 * 32) *m = 64;
+    *m = n > 32 * 32 ? 64 : (n >= 96 ? 32 : 16);
     const int S = (n + *m - 1) / *m;
-    int L = 256 / (S > 0 ? S : 1);
-    if (L > 32) L = 32;
-    if (L < 8) L = 8;
-    int p = 8;
-    while (p * 2 <= L) p *= 2;
-    *lines = p;
+    int L = 32;
+    while (L > 8 && L * S > max_threads_for_m(*m)) L /= 2;
+    *lines = L;
 }
 
 int build_tables(pado_op_s *op)
@@ -103,6 +103,7 @@ int build_tables(pado_op_s *op)
                 std::memcpy(dt.mb, sw.mb, sizeof(dt.mb));
                 std::vector<double> tab, segsum;
                 build_device_table(sw, lay, tab, segsum);
+                dt.interior = interior_info(sw, lay, op->m);
                 int rc_ = upload(op, tab, &dt.tab);
                 if (rc_ == PADO_OK) rc_ = upload(op, segsum, &dt.segsum);
                 if (rc_ != PADO_OK) return rc_;
@@ -122,37 +123,15 @@ int build_tables(pado_op_s *op)
     return PADO_OK;
 }
 
-using KernelFn = void (*)(const KParams);
-
-template <int RK, bool PER, bool ADJ>
-KernelFn pick_m(int m)
-{
-    switch (m) {
-    case 8: return line_kernel<RK, PER, ADJ, 8>;
-    case 16: return line_kernel<RK, PER, ADJ, 16>;
-    case 32: return line_kernel<RK, PER, ADJ, 32>;
-    default: return line_kernel<RK, PER, ADJ, 64>;
-    }
-}
-
-template <int RK>
-KernelFn pick_rk(bool per, bool adj, int m)
-{
-    if (per) return adj ? pick_m<RK, true, true>(m) : pick_m<RK, true, false>(m);
-    return adj ? pick_m<RK, false, true>(m) : pick_m<RK, false, false>(m);
-}
-
-KernelFn pick_kernel(int rk, bool per, bool adj, int m)
+KernelFn pick_kernel(int rk, bool per, bool adj, bool contiguous, int m, int variant)
 {
     switch (rk) {
-    case RHS_CD06_D1: return pick_rk<RHS_CD06_D1>(per, adj, m);
-    case RHS_CD10_D1: return pick_rk<RHS_CD10_D1>(per, adj, m);
-    case RHS_CD10_D2: return pick_rk<RHS_CD10_D2>(per, adj, m);
-    default: return pick_rk<RHS_CF90>(per, adj, m);
+    case RHS_CD06_D1: return pick_kernel_rk0(per, adj, contiguous, m, variant);
+    case RHS_CD10_D1: return pick_kernel_rk1(per, adj, contiguous, m, variant);
+    case RHS_CD10_D2: return pick_kernel_rk2(per, adj, contiguous, m, variant);
+    default: return pick_kernel_rk3(per, adj, contiguous, m, variant);
     }
 }
-
-int max_threads_for_m(int m) { return m >= 64 ? 256 : 512; }
 
 // Geometry of the line family for (axis, na, nb).
 void set_geometry(KParams &kp, int axis, int n, long long na, long long nb)
@@ -216,6 +195,9 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
     std::memcpy(kp.mb, dt.mb, sizeof(kp.mb));
     std::memcpy(kp.taps, dt.taps, sizeof(kp.taps));
     kp.rc = dt.rc;
+    kp.int_mask = dt.interior.mask;
+    std::memcpy(kp.kc, dt.interior.kc, sizeof(kp.kc));
+    std::memcpy(kp.pat, dt.interior.pat, sizeof(kp.pat));
     *kpo = kp;
     *trivial = false;
     return PADO_OK;
@@ -240,15 +222,30 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
     }
     const int threads = kp.L * kp.S;
     if (threads > max_threads_for_m(op->m)) return PADO_E_SIZE;
-    const size_t smem = smem_doubles(kp.L, kp.P, kp.S) * sizeof(double);
-    KernelFn fn = pick_kernel(kp.rc.rk, op->periodic != 0, adjoint, op->m);
-    static std::mutex attr_mu;
+    const bool contiguous = kp.stride == 1;
+    const bool persist = !adjoint && (op->variant == 2 || (op->variant == 3 && !contiguous));
+    const size_t tile = (adjoint || contiguous) ? (size_t)kp.L * kp.P : (op->variant == 2 ? (size_t)kp.n * kp.L : 0);
+    const size_t smem = smem_doubles(kp.L, kp.S, tile) * sizeof(double);
+    if (smem > 227 * 1024) return PADO_E_SIZE;
+    KernelFn fn = pick_kernel(kp.rc.rk, op->periodic != 0, adjoint, contiguous, op->m, op->variant);
+    int per_sm = 1;
     {
+        static std::mutex attr_mu;
         std::lock_guard<std::mutex> g(attr_mu);
         cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cuda_fail(e);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+        if (e != cudaSuccess) return cuda_fail(e);
+        if (per_sm < 1) return PADO_E_SIZE;
     }
-    const long long grid = (kp.nlines + kp.L - 1) / kp.L;
+    const long long ntiles = (kp.nlines + kp.L - 1) / kp.L;
+    long long grid = ntiles;
+    if (persist) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        grid = std::min<long long>(ntiles, (long long)per_sm * sms);
+    }
     if (grid > 0x7fffffffLL) return PADO_E_SIZE;
     fn<<<(unsigned)grid, threads, smem, st>>>(kp);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -375,7 +372,7 @@ int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, doub
 int pado_set_tiling(pado_op_t op, int m, int lines)
 {
     if (!op) return PADO_E_NULL;
-    if (m != 0 && m != 8 && m != 16 && m != 32 && m != 64) return PADO_E_ARG;
+    if (m != 0 && m != 16 && m != 32 && m != 64) return PADO_E_ARG;
     if (lines != 0 && lines != 8 && lines != 16 && lines != 32) return PADO_E_ARG;
     const int om = op->m, ol = op->lines;
     if (m) op->m = m;
@@ -387,6 +384,14 @@ int pado_set_tiling(pado_op_t op, int m, int lines)
         return PADO_E_SIZE;
     }
     if (op->m != om) return build_tables(op);
+    return PADO_OK;
+}
+
+int pado_set_kernel_variant(pado_op_t op, int variant)
+{
+    if (!op) return PADO_E_NULL;
+    if (variant < 0 || variant > 3) return PADO_E_ARG;
+    op->variant = variant == 0 ? 1 : variant;
     return PADO_OK;
 }
 

@@ -15,16 +15,16 @@ constexpr int BATCH_M = 32;  // segment length of the batched kernel
 struct BatchItemDev {
     KParams kp;            // geometry, tables and tiling of this item
     long long tile0;       // first tile index of this item
-    int code;              // rk * 4 + periodic * 2 + adjoint
+    int code;              // rk * 4 + periodic * 2 + direct
     int pad;
 };
 
 #ifdef __CUDACC__
-template <int RK, bool PER, bool ADJ>
+template <int RK, bool PER, bool STRIDED>
 __device__ __forceinline__ void batch_tile(const KParams &kp, double *smem, long long q0)
 {
     const Smem sm = carve(smem, kp.L, kp.P, kp.S);
-    run_tile<RK, PER, ADJ, BATCH_M>(kp, sm, q0);
+    run_tile<RK, PER, false, BATCH_M, STRIDED ? IN_GLOBAL : IN_LINES>(kp, sm, q0);
 }
 
 // counter: tile counter, zeroed before the launch.

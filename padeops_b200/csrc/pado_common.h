@@ -149,13 +149,15 @@ PADO_HD PADO_INLINE double rhs_interior(int rk, int periodic, const double *c, c
 }
 
 // ---------------------------------------------------------------------------
-// One closure row of a bounded line.  `line` is the whole line (stride 1),
+// One closure row of a bounded line.  `line` is the whole line (element
+// stride `stride`),
 // `row` is 0-based and lies in the first or last closure_rows(rk) rows.
 // F(j) below is the reference's 1-based f(j).
 // ---------------------------------------------------------------------------
-PADO_HD inline double rhs_closure_row(int rk, const double *c, const double *line, int n, int row, int bc1, int bcn)
+PADO_HD inline double rhs_closure_row(int rk, const double *c, const double *line, long long stride, int n, int row,
+                                      int bc1, int bcn)
 {
-#define F(j) line[(j)-1]
+#define F(j) line[(long long)((j)-1) * stride]
     const int i = row + 1;  // 1-based
     const bool left = i <= closure_rows(rk);
     switch (rk) {

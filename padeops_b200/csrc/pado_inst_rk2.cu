@@ -1,0 +1,40 @@
+// pado_inst_rk2.cu -- instantiations of the line kernels for one stencil
+// (cd10 second derivative); split per stencil so the library compiles in parallel.
+#include "pado_internal.h"
+
+namespace pado {
+
+namespace {
+
+// variant 1: one CTA per tile; 2: persistent CTAs with cp.async prefetch;
+// 3: persistent CTAs reading straight from global memory with an L2 prefetch.
+// The adjoint always runs one CTA per tile.
+template <bool PER, int M>
+KernelFn pick_in(bool adj, bool contiguous, int variant)
+{
+    constexpr int RK = 2;
+    if (adj) return contiguous ? line_kernel<RK, PER, true, M, IN_LINES> : line_kernel<RK, PER, true, M, IN_GLOBAL>;
+    if (variant == 2)
+        return contiguous ? line_kernel_persist<RK, PER, M, IN_LINES> : line_kernel_persist<RK, PER, M, IN_ROWS>;
+    if (variant == 3 && !contiguous) return line_kernel_persist<RK, PER, M, IN_GLOBAL>;
+    return contiguous ? line_kernel<RK, PER, false, M, IN_LINES> : line_kernel<RK, PER, false, M, IN_GLOBAL>;
+}
+
+template <bool PER>
+KernelFn pick_m(int m, bool adj, bool contiguous, int variant)
+{
+    switch (m) {
+    case 16: return pick_in<PER, 16>(adj, contiguous, variant);
+    case 32: return pick_in<PER, 32>(adj, contiguous, variant);
+    default: return pick_in<PER, 64>(adj, contiguous, variant);
+    }
+}
+
+}  // namespace
+
+KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant)
+{
+    return per ? pick_m<true>(m, adj, contiguous, variant) : pick_m<false>(m, adj, contiguous, variant);
+}
+
+}  // namespace pado

@@ -27,6 +27,7 @@ struct DevTables {
     int nb = 0, nbord = 0;
     Layout lay;
     RhsCoef rc{};
+    Interior interior;  // constant-coefficient segments for tiling m
 };
 
 using TabKey = std::tuple<int, int, int, int>;  // kind, bc1, bcn, adjoint
@@ -41,6 +42,7 @@ struct pado_op_s {
     int scheme = 0, n = 0, periodic = 1, bc1 = 0, bcn = 0;
     double dx = 1.0;
     int m = 32, lines = 16;
+    int variant = 1;  // 1: one CTA per tile, 2: persistent CTAs with cp.async prefetch
     int device = 0;
     std::map<pado::TabKey, pado::DevTables> tables;
     std::vector<void *> allocations;
@@ -55,6 +57,13 @@ namespace pado {
 // Validates an apply request and fills the launch parameters for the given
 // lines-per-CTA.  Returns PADO_OK, or an error; *trivial is set when n == 1
 // or the field is empty (nothing for a line kernel to do).
+// Line-kernel entry points, one translation unit per stencil (pado_inst_rk*.cu).
+using KernelFn = void (*)(const KParams);
+KernelFn pick_kernel_rk0(bool per, bool adj, bool contiguous, int m, int variant);
+KernelFn pick_kernel_rk1(bool per, bool adj, bool contiguous, int m, int variant);
+KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant);
+KernelFn pick_kernel_rk3(bool per, bool adj, bool contiguous, int m, int variant);
+
 int prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
                    int bcn, bool adjoint, int lines, KParams *kp, bool *trivial);
 

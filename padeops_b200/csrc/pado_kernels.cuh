@@ -1,25 +1,35 @@
 // pado_kernels.cuh -- the line kernel: explicit stencil fused with the banded
 // solve, for one line family (all lines of a field along one axis).
 //
-// A CTA owns a tile of L lines (lanes) and cuts every line into S segments
-// (thread (l, s) = lane l, segment s).  Per tile:
+// A CTA owns a tile of L lines and cuts every line into S segments; thread
+// (l, s) = line lane l (fastest), segment s.  Lanes are lines, so for lines
+// along a strided axis (y, z) a warp's accesses to one row are contiguous in
+// memory.  The input of a tile comes from one of three places (IN):
+//   IN_GLOBAL  straight from global memory into registers (strided lines)
+//   IN_ROWS    a shared-memory tile [n][L] (strided lines), filled by cp.async
+//   IN_LINES   a shared-memory tile [L][P], P odd (contiguous x lines)
+// and results go straight from registers to global memory.  The persistent
+// kernel prefetches the next tile with cp.async while the current one runs
+// its chains and backward sweep.  Per tile:
 //
-//   load     the L x n tile into shared memory (pitch P = odd, so lane-strided
-//            accesses are bank-conflict free)
 //   fwd      stencil rows of the segment (reference grouping), then the local
-//            forward recurrence with zero incoming state, kept in registers
-//   chainF   one thread per line walks the S segments: incoming states,
-//            cyclic border unknowns
+//            forward recurrence with zero incoming state, in registers
+//   chainF   one thread per line walks the S segments: incoming states and
+//            the cyclic border unknowns
 //   bwd      local backward recurrence (forward values corrected on the fly)
 //   chainB   one thread per line walks the segments backwards
-//   fin      x = local + incoming-state corrections -> tile -> global
+//   fin      x = local + incoming-state corrections -> df
 //
 // The adjoint kernel runs the transposed sweep first and the transposed
-// stencil last.  Each phase is a __host__ __device__ function so tests can
-// run the same code on the CPU.
+// stencil last (through the tile).  Each phase is a __host__ __device__
+// function so the tests run the same code on the CPU.
 #pragma once
 
 #include "pado_common.h"
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#endif
 
 namespace pado {
 
@@ -41,6 +51,10 @@ struct KParams {
     double mb[4];
     double taps[9];        // adjoint: interior transposed taps
     RhsCoef rc;
+    // constant-coefficient interior (see Interior in pado_tables.h)
+    unsigned int_mask;     // bit s: segment s takes the register-only path
+    double kc[8];          // alpha, c1, c2, gamma, d1, d2, delta
+    double pat[8];         // U(m-1), V(m-1), U(m-2), V(m-2), S(0), T(0), S(1), T(1)
 };
 
 PADO_HD PADO_INLINE int seg_start(const KParams &kp, int s) { return s * kp.base + (s < kp.rem ? s : kp.rem); }
@@ -50,97 +64,119 @@ PADO_HD PADO_INLINE long long line_base(const KParams &kp, long long q)
     return (q % kp.line_ia) + (q / kp.line_ia) * kp.line_oc;
 }
 
-// Shared-memory carve-up (doubles).
+// Shared-memory carve-up (doubles).  The tile is only allocated by kernels
+// that use it (x lines, and every adjoint).
 struct Smem {
-    double *tile;  // [L][P]
     double *buf4;  // [S][L][4]  forward summaries, later backward summaries
     double *buf2;  // [S][L][2]  forward incoming states, later backward ones
     double *eb;    // [L][4]     border unknowns E (0..1) and border rhs (2..3)
+    double *tile;  // [L][P]
 };
 
-PADO_HD PADO_INLINE size_t smem_doubles(int L, int P, int S) { return (size_t)L * P + (size_t)S * L * 6 + (size_t)L * 4; }
+// tile_doubles: 0 (no tile), L*P ([L][P] tile) or n*L ([n][L] tile)
+PADO_HD PADO_INLINE size_t smem_doubles(int L, int S, size_t tile_doubles)
+{
+    return (size_t)S * L * 6 + (size_t)L * 4 + tile_doubles;
+}
 
 PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S)
 {
     Smem sm;
-    sm.tile = base;
-    sm.buf4 = sm.tile + (size_t)L * P;
+    sm.buf4 = base;
     sm.buf2 = sm.buf4 + (size_t)S * L * 4;
     sm.eb = sm.buf2 + (size_t)S * L * 2;
+    sm.tile = sm.eb + (size_t)L * 4;
+    (void)P;
     return sm;
 }
 
+// Per-thread segment values: M rows plus the 8-row stencil window margin.
 template <int M>
 struct Regs {
-    double r[M];
+    double r[M + 8];
+};
+
+struct Dbl2 {
+    double x, y;
 };
 
 #ifdef __CUDA_ARCH__
 #define PADO_LDG(p) __ldg(p)
+__device__ __forceinline__ Dbl2 ldg2(const double *p)
+{
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    return Dbl2{v.x, v.y};
+}
 #else
 #define PADO_LDG(p) (*(p))
+inline Dbl2 ldg2(const double *p) { return Dbl2{p[0], p[1]}; }
 #endif
 
 // ---------------------------------------------------------------------------
-// Tile load / store (cooperative over the CTA's nthreads threads).
+// Tile load / store for contiguous lines (x): the L lines of a tile are one
+// contiguous run of L*n doubles; all threads stream it with independent loads.
 // ---------------------------------------------------------------------------
 PADO_HD PADO_INLINE void tile_load(const KParams &kp, const Smem &sm, long long q0, int tid, int nthreads)
 {
     const int n = kp.n, L = kp.L, P = kp.P;
-    if (kp.stride == 1) {
-        // lines contiguous: stream each line with all threads
-        for (int l = 0; l < L; ++l) {
-            const long long q = q0 + l;
-            if (q >= kp.nlines) break;
-            const double *src = kp.in + line_base(kp, q);
-            double *dst = sm.tile + (size_t)l * P;
-            for (int r = tid; r < n; r += nthreads) dst[r] = src[r];
+    const int nl = (int)(kp.nlines - q0 < L ? kp.nlines - q0 : L);
+    const int total = nl * n;
+    const double *src = kp.in + line_base(kp, q0);
+    // element e = tid + k*nthreads sits at (line l, row r); advance (l, r) without divisions
+    int l = tid / n, r = tid - (tid / n) * n;
+    const int dl = nthreads / n, dr = nthreads - dl * n;
+    for (int e = tid; e < total; e += 4 * nthreads) {
+        double v[4];
+        int ls[4], rs[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int ee = e + u * nthreads;
+            v[u] = ee < total ? src[ee] : 0.0;
+            ls[u] = l;
+            rs[u] = r;
+            l += dl;
+            r += dr;
+            if (r >= n) {
+                r -= n;
+                ++l;
+            }
         }
-    } else {
-        // strided lines: lanes read consecutive lines (coalesced) row by row
-        const int l = tid % L, s = tid / L, S = nthreads / L;
-        const long long q = q0 + l;
-        if (s < S && q < kp.nlines) {
-            const double *src = kp.in + line_base(kp, q);
-            double *dst = sm.tile + (size_t)l * P;
-            for (int r = s; r < n; r += S) dst[r] = src[(long long)r * kp.stride];
-        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (e + u * nthreads < total) sm.tile[(size_t)ls[u] * P + rs[u]] = v[u];
     }
 }
 
 PADO_HD PADO_INLINE void tile_store(const KParams &kp, const Smem &sm, long long q0, int tid, int nthreads)
 {
     const int n = kp.n, L = kp.L, P = kp.P;
-    if (kp.stride == 1) {
-        for (int l = 0; l < L; ++l) {
-            const long long q = q0 + l;
-            if (q >= kp.nlines) break;
-            double *dst = kp.out + line_base(kp, q);
-            const double *src = sm.tile + (size_t)l * P;
-            for (int r = tid; r < n; r += nthreads) dst[r] = src[r];
-        }
-    } else {
-        const int l = tid % L, s = tid / L, S = nthreads / L;
-        const long long q = q0 + l;
-        if (s < S && q < kp.nlines) {
-            double *dst = kp.out + line_base(kp, q);
-            const double *src = sm.tile + (size_t)l * P;
-            for (int r = s; r < n; r += S) dst[(long long)r * kp.stride] = src[r];
+    const int nl = (int)(kp.nlines - q0 < L ? kp.nlines - q0 : L);
+    const int total = nl * n;
+    double *dst = kp.out + line_base(kp, q0);
+    int l = tid / n, r = tid - (tid / n) * n;
+    const int dl = nthreads / n, dr = nthreads - dl * n;
+    for (int e = tid; e < total; e += nthreads) {
+        dst[e] = sm.tile[(size_t)l * P + r];
+        l += dl;
+        r += dr;
+        if (r >= n) {
+            r -= n;
+            ++l;
         }
     }
 }
 
 // Closure rows are rare (first/last few rows of a bounded line): evaluate
-// them out of line from the tile.
+// them out of line from memory (the tile, or global memory with a stride).
 #ifdef __CUDA_ARCH__
 __device__ __noinline__
 #else
 inline
 #endif
     double
-    closure_row_noinline(const RhsCoef &rc, const double *line, int n, int row, int bc1, int bcn)
+    closure_row_noinline(const RhsCoef *rc, const double *line, long long stride, int n, int row, int bc1, int bcn)
 {
-    return rhs_closure_row(rc.rk, rc.c, line, n, row, bc1, bcn);
+    return rhs_closure_row(rc->rk, rc->c, line, stride, n, row, bc1, bcn);
 }
 
 // Transposed stencil at one column j of a bounded line from explicit blocks.
@@ -168,50 +204,167 @@ inline
     return acc;
 }
 
-template <int RK, bool PER, bool ADJ, int M>
+enum InputSource { IN_GLOBAL = 0, IN_ROWS = 1, IN_LINES = 2 };
+
+template <int RK, bool PER, bool ADJ, int M, int IN>
 struct LineKernel {
     static constexpr bool CYC = PER;
+    static constexpr bool ORDER2 = RK != RHS_CD06_D1;  // tridiagonal (cd06) sweeps have no second lag
+    // only the bounded cd06 (Thomas) sweep scales its input (alpha != 1), and
+    // only its adjoint scales the output (delta != 1)
+    static constexpr bool HAS_ALPHA = RK == RHS_CD06_D1 && !PER && !ADJ;
+    static constexpr bool HAS_DELTA = RK == RHS_CD06_D1 && !PER && ADJ;
 
-    // value of the tile line at row (wrapped when periodic, 0 outside when bounded)
-    static PADO_HD PADO_INLINE double tv(const double *line, int n, int row)
+    static PADO_HD PADO_INLINE bool fast(const KParams &kp, int s) { return (kp.int_mask >> s) & 1u; }
+
+    // ---- constant-coefficient interior segment: stencil + forward sweep ----
+    static PADO_HD PADO_INLINE void fwd_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s,
+                                             const double *gline, long long gs)
     {
-        if (PER) {
-            row = row < 0 ? row + n : (row >= n ? row - n : row);
-            return line[row];
+        const int a = seg_start(kp, s);
+        if (!ADJ) {
+            const double *p = gline + (long long)(a - 4) * gs;
+#pragma unroll
+            for (int j = 0; j < M + 8; ++j) R.r[j] = p[(long long)j * gs];
+#pragma unroll
+            for (int t = 0; t < M; ++t) R.r[t] = rhs_interior(RK, PER, kp.rc.c, &R.r[t]);
+        } else {
+            const double *p = gline + (long long)a * gs;
+#pragma unroll
+            for (int t = 0; t < M; ++t) R.r[t] = p[(long long)t * gs];
         }
-        return (row >= 0 && row < n) ? line[row] : 0.0;
+        const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
+        double z1 = 0.0, z2 = 0.0;
+#pragma unroll
+        for (int t = 0; t < M; ++t) {
+            double z = HAS_ALPHA ? al * R.r[t] : R.r[t];
+            if (ORDER2) z -= c2 * z2;
+            z -= c1 * z1;
+            R.r[t] = z;
+            z2 = z1;
+            z1 = z;
+        }
+        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
+        o[0] = z1;
+        o[1] = z2;
+        o[2] = 0.0;
+        o[3] = 0.0;
     }
 
+    // ---- constant-coefficient interior segment: backward sweep -------------
+    static PADO_HD PADO_INLINE void bwd_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
+    {
+        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
+        const double c1 = kp.kc[1], c2 = kp.kc[2], ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
+        // forward values: local solution + homogeneous solution from the incoming state
+        double h1 = st[0], h2 = st[1];
+#pragma unroll
+        for (int t = 0; t < M; ++t) {
+            double h = -c1 * h1;
+            if (ORDER2) h -= c2 * h2;
+            R.r[t] += h;
+            h2 = h1;
+            h1 = h;
+        }
+        double x1 = 0.0, x2 = 0.0;
+#pragma unroll
+        for (int t = M - 1; t >= 0; --t) {
+            double x = ga * R.r[t];
+            if (ORDER2) x -= d2 * x2;
+            x -= d1 * x1;
+            R.r[t] = x;
+            x2 = x1;
+            x1 = x;
+        }
+        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
+        o[0] = x1;
+        o[1] = x2;
+    }
+
+    // ---- constant-coefficient interior segment: corrections + output ------
+    static PADO_HD PADO_INLINE void fin_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s,
+                                             double *line, long long gs)
+    {
+        const int a = seg_start(kp, s);
+        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
+        const double d1 = kp.kc[4], d2 = kp.kc[5], de = kp.kc[6];
+        double g1 = st[0], g2 = st[1];
+        double *p = line + (long long)a * gs;
+#pragma unroll
+        for (int t = M - 1; t >= 0; --t) {
+            double g = -d1 * g1;
+            if (ORDER2) g -= d2 * g2;
+            double x = R.r[t] + g;
+            if (HAS_DELTA) x *= de;
+            p[(long long)t * gs] = x;
+            g2 = g1;
+            g1 = g;
+        }
+    }
+
+    static PADO_HD PADO_INLINE int wrap(int row, int n) { return row < 0 ? row + n : (row >= n ? row - n : row); }
+
     // ---- phase fwd: right-hand side (primal) + local forward sweep ---------
-    static PADO_HD PADO_INLINE void fwd(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
+    static PADO_HD PADO_INLINE void fwd(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, long long q0)
     {
         const int n = kp.n, nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;  // banded rows of this segment
-        const double *line = sm.tile + (size_t)l * kp.P;
+        const long long q = q0 + l;
+        const bool live = q < kp.nlines;
+        // source line: global (strided), a tile column [n][L] or a tile row [L][P]
+        const double *gline = IN == IN_GLOBAL ? kp.in + line_base(kp, live ? q : 0)
+                            : IN == IN_ROWS   ? sm.tile + l
+                                              : sm.tile + (size_t)l * kp.P;
+        const long long gs = IN == IN_GLOBAL ? kp.stride : IN == IN_ROWS ? kp.L : 1;
+        if (fast(kp, s)) {
+            fwd_fast(kp, sm, R, l, s, gline, gs);
+            return;
+        }
         if (!ADJ) {
-            // sliding 9-point window over the tile row
-            double v[9];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k + 1] = tv(line, n, a - 4 + k);
+            // Closure rows of a bounded line (first/last segment only) are
+            // evaluated first, out of line, while few registers are live.
             const int cr = closure_rows(RK);
+            double cv[4] = {0.0, 0.0, 0.0, 0.0};
+            const bool first = !PER && s == 0, last = !PER && s == kp.S - 1;
+            if (first || last) {
+                for (int k = 0; k < cr; ++k) {
+                    if (live && first) cv[k] = closure_row_noinline(&kp.rc, gline, gs, n, k, kp.bc1, kp.bcn);
+                }
+            }
+            double cl[4] = {0.0, 0.0, 0.0, 0.0};
+            if (last) {
+                for (int k = 0; k < cr; ++k)
+                    if (live) cl[k] = closure_row_noinline(&kp.rc, gline, gs, n, n - cr + k, kp.bc1, kp.bcn);
+            }
+            // window rows a-4 .. a+len+3, all loads issued up front; the
+            // stencil result of row t overwrites R.r[t], the oldest window entry
 #pragma unroll
-            for (int t = 0; t < M; ++t) {
+            for (int j = 0; j < M + 8; ++j) {
+                const int row = a - 4 + j;
+                const bool ok = live && j < len + 8 && (PER || (row >= 0 && row < n));
+                R.r[j] = ok ? gline[(long long)(PER ? wrap(row, n) : row) * gs] : 0.0;
+            }
 #pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] = v[k + 1];
-                v[8] = t < len ? tv(line, n, a + t + 4) : 0.0;
-                if (t < len) {
-                    const int row = a + t;
-                    if (!PER && (row < cr || row >= n - cr))
-                        R.r[t] = closure_row_noinline(kp.rc, line, n, row, kp.bc1, kp.bcn);
-                    else
-                        R.r[t] = rhs_interior(RK, PER, kp.rc.c, v);
+            for (int t = 0; t < M; ++t)
+                if (t < len) R.r[t] = rhs_interior(RK, PER, kp.rc.c, &R.r[t]);
+            if (first) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (k < cr && k < len) R.r[k] = cv[k];
+            }
+            if (last) {
+#pragma unroll
+                for (int t = 0; t < M; ++t) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (k < cr && t == len - cr + k) R.r[t] = cl[k];
                 }
             }
         } else {
 #pragma unroll
             for (int t = 0; t < M; ++t)
-                if (t < len) R.r[t] = line[a + t];
+                if (t < len) R.r[t] = live ? gline[(long long)(a + t) * gs] : 0.0;
         }
         // local forward sweep with zero incoming state
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -220,12 +373,15 @@ struct LineKernel {
         for (int t = 0; t < M; ++t) {
             if (t < lenb) {
                 const double *tr = tb + (size_t)t * T_NF;
-                const double c1 = PADO_LDG(tr + T_C1), c2 = PADO_LDG(tr + T_C2), al = PADO_LDG(tr + T_ALPHA);
-                const double z = (al * R.r[t] - c2 * z2) - c1 * z1;
+                const Dbl2 cc = ldg2(tr + T_C1);
+                const Dbl2 ak = (HAS_ALPHA || CYC) ? ldg2(tr + T_ALPHA) : Dbl2{1.0, 0.0};
+                double z = HAS_ALPHA ? ak.x * R.r[t] : R.r[t];
+                if (ORDER2) z -= cc.y * z2;
+                z -= cc.x * z1;
                 R.r[t] = z;
                 if (CYC) {
-                    s1 += PADO_LDG(tr + T_K1) * z;
-                    s2 += PADO_LDG(tr + T_K2) * z;
+                    s1 += ak.y * z;
+                    if (ORDER2) s2 += PADO_LDG(tr + T_K2) * z;
                 }
                 z2 = z1;
                 z1 = z;
@@ -253,23 +409,26 @@ struct LineKernel {
     static PADO_HD PADO_INLINE void chain_fwd(const KParams &kp, const Smem &sm, int l)
     {
         double P1 = 0.0, P2 = 0.0, sg1 = 0.0, sg2 = 0.0;
-        for (int s = 0; s < kp.S; ++s) {
+        const int S = kp.S;
+#pragma unroll 4
+        for (int s = 0; s < S; ++s) {
             const double *in4 = sm.buf4 + ((size_t)s * kp.L + l) * 4;
-            const double zl = in4[0], zl2 = in4[1], ps1 = in4[2], ps2 = in4[3];
+            const double zl = in4[0], zl2 = in4[1];
             double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
             st[0] = P1;
             st[1] = P2;
             if (CYC) {
-                const double *ss = kp.segsum + (size_t)s * 4;
-                sg1 += ps1 + P1 * PADO_LDG(ss + 0) + P2 * PADO_LDG(ss + 1);
-                sg2 += ps2 + P1 * PADO_LDG(ss + 2) + P2 * PADO_LDG(ss + 3);
+                const Dbl2 s01 = ldg2(kp.segsum + (size_t)s * 4), s23 = ldg2(kp.segsum + (size_t)s * 4 + 2);
+                sg1 += in4[2] + P1 * s01.x + P2 * s01.y;
+                sg2 += in4[3] + P1 * s23.x + P2 * s23.y;
             }
-            if (s + 1 < kp.S) {
-                const int a = seg_start(kp, s), len = seg_len(kp, s);
-                const int b = (a + len <= kp.nb) ? a + len : kp.nb;
-                const double *t1 = kp.tab + (size_t)(b - 1) * T_NF, *t2 = kp.tab + (size_t)(b - 2) * T_NF;
-                const double n1 = zl + P1 * PADO_LDG(t1 + T_U) + P2 * PADO_LDG(t1 + T_V);
-                const double n2 = zl2 + P1 * PADO_LDG(t2 + T_U) + P2 * PADO_LDG(t2 + T_V);
+            if (s + 1 < S) {
+                const int b = seg_start(kp, s + 1);  // segments before the last are fully banded
+                const bool f = fast(kp, s);
+                const Dbl2 uv1 = f ? Dbl2{kp.pat[0], kp.pat[1]} : ldg2(kp.tab + (size_t)(b - 1) * T_NF + T_U);
+                const Dbl2 uv2 = f ? Dbl2{kp.pat[2], kp.pat[3]} : ldg2(kp.tab + (size_t)(b - 2) * T_NF + T_U);
+                const double n1 = zl + P1 * uv1.x + P2 * uv1.y;
+                const double n2 = zl2 + P1 * uv2.x + P2 * uv2.y;
                 P1 = n1;
                 P2 = n2;
             }
@@ -290,6 +449,10 @@ struct LineKernel {
     // ---- phase bwd: local backward sweep ---------------------------------
     static PADO_HD PADO_INLINE void bwd(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
     {
+        if (fast(kp, s)) {
+            bwd_fast(kp, sm, R, l, s);
+            return;
+        }
         const int nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;
@@ -306,10 +469,18 @@ struct LineKernel {
         for (int t = M - 1; t >= 0; --t) {
             if (t < lenb) {
                 const double *tr = tb + (size_t)t * T_NF;
-                const double z = R.r[t] + P1 * PADO_LDG(tr + T_U) + P2 * PADO_LDG(tr + T_V);
-                double x = PADO_LDG(tr + T_GAMMA) * z;
-                if (CYC) x = x - PADO_LDG(tr + T_E2) * E2 - PADO_LDG(tr + T_E1) * E1;
-                x = x - PADO_LDG(tr + T_D2) * x2 - PADO_LDG(tr + T_D1) * x1;
+                const Dbl2 uv = ldg2(tr + T_U);
+                const Dbl2 gd = ldg2(tr + T_GAMMA);
+                const Dbl2 de = ldg2(tr + T_D2);
+                double z = R.r[t] + P1 * uv.x;
+                if (ORDER2) z += P2 * uv.y;
+                double x = gd.x * z;
+                if (CYC) {
+                    x -= de.y * E1;
+                    if (ORDER2) x -= PADO_LDG(tr + T_E2) * E2;
+                }
+                if (ORDER2) x -= de.x * x2;
+                x -= gd.y * x1;
                 R.r[t] = x;
                 x2 = x1;
                 x1 = x;
@@ -324,6 +495,7 @@ struct LineKernel {
     static PADO_HD PADO_INLINE void chain_bwd(const KParams &kp, const Smem &sm, int l)
     {
         double Q1 = 0.0, Q2 = 0.0;
+#pragma unroll 4
         for (int s = kp.S - 1; s >= 0; --s) {
             const double *in4 = sm.buf4 + ((size_t)s * kp.L + l) * 4;
             double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
@@ -331,17 +503,22 @@ struct LineKernel {
             st[1] = Q2;
             if (s > 0) {
                 const int a = seg_start(kp, s);
-                const double *t0 = kp.tab + (size_t)a * T_NF, *t1 = kp.tab + (size_t)(a + 1) * T_NF;
-                const double n1 = in4[0] + Q1 * PADO_LDG(t0 + T_S) + Q2 * PADO_LDG(t0 + T_T);
-                const double n2 = in4[1] + Q1 * PADO_LDG(t1 + T_S) + Q2 * PADO_LDG(t1 + T_T);
+                const bool f = fast(kp, s);
+                const Dbl2 st0 = f ? Dbl2{kp.pat[4], kp.pat[5]} : ldg2(kp.tab + (size_t)a * T_NF + T_S);
+                const Dbl2 st1 = f ? Dbl2{kp.pat[6], kp.pat[7]} : ldg2(kp.tab + (size_t)(a + 1) * T_NF + T_S);
+                const double n1 = in4[0] + Q1 * st0.x + Q2 * st0.y;
+                const double n2 = in4[1] + Q1 * st1.x + Q2 * st1.y;
                 Q1 = n1;
                 Q2 = n2;
             }
         }
     }
 
-    // ---- phase fin: corrected values -> tile ------------------------------
-    static PADO_HD PADO_INLINE void fin(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
+    // ---- phase fin: corrected values -> df (primal) or the tile (adjoint) --
+    // OUT_TILE: write the result into the [L][P] tile (adjoint, and x lines
+    // whose tile is then stored with coalesced accesses) instead of global memory
+    template <bool OUT_TILE = ADJ>
+    static PADO_HD PADO_INLINE void fin(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, long long q0)
     {
         const int nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
@@ -349,19 +526,29 @@ struct LineKernel {
         const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
         const double Q1 = st[0], Q2 = st[1];
         const double *tb = kp.tab + (size_t)a * T_NF;
-        double *line = sm.tile + (size_t)l * kp.P;
+        const long long q = q0 + l;
+        const bool to_global = !OUT_TILE;
+        if (to_global && q >= kp.nlines) return;
+        double *line = to_global ? kp.out + line_base(kp, q) : sm.tile + (size_t)l * kp.P;
+        const long long gs = to_global ? kp.stride : 1;
+        if (fast(kp, s)) {
+            fin_fast(kp, sm, R, l, s, line, gs);
+            return;
+        }
 #pragma unroll
         for (int t = 0; t < M; ++t) {
             if (t < lenb) {
                 const double *tr = tb + (size_t)t * T_NF;
-                double x = R.r[t] + Q1 * PADO_LDG(tr + T_S) + Q2 * PADO_LDG(tr + T_T);
-                if (ADJ) x = PADO_LDG(tr + T_DELTA) * x;
-                line[a + t] = x;
+                const Dbl2 stt = ldg2(tr + T_S);
+                double x = R.r[t] + Q1 * stt.x;
+                if (ORDER2) x += Q2 * stt.y;
+                if (HAS_DELTA) x = PADO_LDG(tr + T_DELTA) * x;
+                line[(long long)(a + t) * gs] = x;
             }
         }
         if (CYC && s == kp.S - 1) {
-            line[nb] = sm.eb[(size_t)l * 4 + 0];
-            if (kp.nbord == 2) line[nb + 1] = sm.eb[(size_t)l * 4 + 1];
+            line[(long long)nb * gs] = sm.eb[(size_t)l * 4 + 0];
+            if (kp.nbord == 2) line[(long long)(nb + 1) * gs] = sm.eb[(size_t)l * 4 + 1];
         }
     }
 
@@ -371,96 +558,242 @@ struct LineKernel {
         const int n = kp.n;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const double *line = sm.tile + (size_t)l * kp.P;
-        double v[9];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k + 1] = tv(line, n, a - 4 + k);
         const int zone = n <= 32 ? n : 8;
 #pragma unroll
+        for (int j = 0; j < M + 8; ++j) {
+            const int row = a - 4 + j;
+            const bool ok = j < len + 8 && (PER || (row >= 0 && row < n));
+            R.r[j] = ok ? line[PER ? wrap(row, n) : row] : 0.0;
+        }
+#pragma unroll
         for (int t = 0; t < M; ++t) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = v[k + 1];
-            v[8] = t < len ? tv(line, n, a + t + 4) : 0.0;
             if (t < len) {
-                const int j = a + t;
-                if (!PER && (j < zone || j >= n - zone)) {
-                    R.r[t] = bt_column_noinline(kp.bt, line, n, j);
-                } else {
-                    double acc = 0.0;
+                double acc = 0.0;
 #pragma unroll
-                    for (int k = 0; k < 9; ++k) acc += kp.taps[k] * v[k];
-                    R.r[t] = acc;
-                }
+                for (int k = 0; k < 9; ++k) acc += kp.taps[k] * R.r[t + k];
+                R.r[t] = acc;
+            }
+        }
+        if (!PER && (a < zone || a + len > n - zone)) {
+            // boundary columns of B^T (explicit blocks), rare: first/last segments
+#pragma unroll
+            for (int t = 0; t < M; ++t) {
+                const int j = a + t;
+                if (t < len && (j < zone || j >= n - zone)) R.r[t] = bt_column_noinline(kp.bt, line, n, j);
             }
         }
     }
 
-    static PADO_HD PADO_INLINE void adj_write(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
+    // ---- phase adjoint output ----------------------------------------------
+    static PADO_HD PADO_INLINE void adj_out(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, long long q0)
     {
         const int a = seg_start(kp, s), len = seg_len(kp, s);
-        double *line = sm.tile + (size_t)l * kp.P;
+        const long long q = q0 + l;
+        if (q >= kp.nlines) return;
+        double *line = kp.out + line_base(kp, q);
+        const long long gs = kp.stride;
 #pragma unroll
         for (int t = 0; t < M; ++t)
-            if (t < len) line[a + t] = R.r[t];
+            if (t < len) line[(long long)(a + t) * gs] = R.r[t];
     }
 };
 
+// Phase schedule of one tile.  Phases are separated by a CTA barrier.
+enum Phase {
+    PH_LOAD = 0, PH_FWD, PH_CHAINF, PH_BWD, PH_CHAINB, PH_FIN, PH_ADJ_STENCIL, PH_ADJ_OUT, PH_STORE, NPHASES
+};
+
+// x lines (IN_LINES) load and store their tile cooperatively; the adjoint
+// runs its transposed stencil after the solve
+template <bool ADJ, int IN>
+PADO_HD PADO_INLINE constexpr bool phase_used(int ph)
+{
+    return (ph == PH_LOAD || ph == PH_STORE) ? IN == IN_LINES && !(ph == PH_STORE && ADJ)
+         : (ph == PH_ADJ_STENCIL || ph == PH_ADJ_OUT) ? ADJ
+         : true;
+}
+
 // One tile of kp.L lines on a CTA of nthreads threads (nthreads >= L*S;
-// the extra threads only help with the tile load/store).
-template <int RK, bool PER, bool ADJ, int M>
+// extra threads only help with the tile load).
+template <int RK, bool PER, bool ADJ, int M, int IN>
 PADO_HD PADO_INLINE void tile_phase(int phase, const KParams &kp, const Smem &sm, Regs<M> &R, long long q0, int tid,
                                     int nthreads)
 {
-    using K = LineKernel<RK, PER, ADJ, M>;
+    using K = LineKernel<RK, PER, ADJ, M, IN>;
     const int l = tid % kp.L, s = tid / kp.L;
     const bool active = s < kp.S;
     switch (phase) {
-    case 0: tile_load(kp, sm, q0, tid, nthreads); break;
-    case 1: if (active) K::fwd(kp, sm, R, l, s); break;
-    case 2: if (s == 0) K::chain_fwd(kp, sm, l); break;
-    case 3: if (active) K::bwd(kp, sm, R, l, s); break;
-    case 4: if (s == 0) K::chain_bwd(kp, sm, l); break;
-    case 5: if (active) K::fin(kp, sm, R, l, s); break;
-    case 6: if (ADJ && active) K::adj_stencil(kp, sm, R, l, s); break;
-    case 7: if (ADJ && active) K::adj_write(kp, sm, R, l, s); break;
+    case PH_LOAD: tile_load(kp, sm, q0, tid, nthreads); break;
+    case PH_FWD: if (active) K::fwd(kp, sm, R, l, s, q0); break;
+    case PH_CHAINF: if (s == 0) K::chain_fwd(kp, sm, l); break;
+    case PH_BWD: if (active) K::bwd(kp, sm, R, l, s); break;
+    case PH_CHAINB: if (s == 0) K::chain_bwd(kp, sm, l); break;
+    case PH_FIN: if (active) K::template fin<ADJ || IN == IN_LINES>(kp, sm, R, l, s, q0); break;
+    case PH_ADJ_STENCIL: if (active) K::adj_stencil(kp, sm, R, l, s); break;
+    case PH_ADJ_OUT: if (active) K::adj_out(kp, sm, R, l, s, q0); break;
     default: tile_store(kp, sm, q0, tid, nthreads); break;
     }
 }
-constexpr int NPHASES = 9;
+
+// ---------------------------------------------------------------------------
+// Asynchronous tile prefetch (persistent kernel).  Each thread copies its
+// share of the tile with 8-byte cp.async; on the host it is a plain copy.
+// ---------------------------------------------------------------------------
+PADO_HD PADO_INLINE void copy8_async(double *dst_smem, const double *src)
+{
+#ifdef __CUDA_ARCH__
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+#else
+    *dst_smem = *src;
+#endif
+}
+PADO_HD PADO_INLINE void copy_async_commit()
+{
+#ifdef __CUDA_ARCH__
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
+PADO_HD PADO_INLINE void copy_async_wait_all()
+{
+#ifdef __CUDA_ARCH__
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+#endif
+}
+
+PADO_HD PADO_INLINE void prefetch_l2(const void *p)
+{
+#ifdef __CUDA_ARCH__
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+#else
+    (void)p;
+#endif
+}
+
+template <int IN>
+PADO_HD PADO_INLINE void tile_prefetch(const KParams &kp, const Smem &sm, long long q0, int tid, int nthreads)
+{
+    const int n = kp.n, L = kp.L;
+    if (IN == IN_GLOBAL) {
+        // strided lines read straight into registers: warm L2 with the tile's
+        // rows (each row of L lines is contiguous when the lines are)
+        const long long nl = kp.nlines - q0 < L ? kp.nlines - q0 : L;
+        if (nl <= 0) return;
+        const double *first = kp.in + line_base(kp, q0), *last = kp.in + line_base(kp, q0 + nl - 1);
+        const long long span = (long long)(last - first) + 1;  // doubles from the first to the last line of a row
+        const int per_row = (int)((span * 8 + 127) / 128);
+        if (per_row > 8) {
+            // lines not adjacent: one prefetch per line and row
+            for (long long e = tid; e < nl * n; e += nthreads) {
+                const long long l = e % nl, r = e / nl;
+                prefetch_l2(kp.in + line_base(kp, q0 + l) + r * kp.stride);
+            }
+            return;
+        }
+        for (int e = tid; e < n * per_row; e += nthreads) {
+            const int r = e / per_row, c = e - r * per_row;
+            prefetch_l2(reinterpret_cast<const char *>(first + (long long)r * kp.stride) + c * 128);
+        }
+        return;
+    }
+    if (IN == IN_ROWS) {
+        // thread (l, s) copies rows s, s+Sn, ... of line l; lanes read consecutive lines
+        const int l = tid % L, s0 = tid / L, Sn = nthreads / L;
+        const long long q = q0 + l;
+        if (s0 >= Sn || q >= kp.nlines) return;
+        const double *src = kp.in + line_base(kp, q);
+        for (int r = s0; r < n; r += Sn) copy8_async(sm.tile + (size_t)r * L + l, src + (long long)r * kp.stride);
+    } else {
+        // the tile's lines are one contiguous run of nl*n doubles
+        const int P = kp.P;
+        const int nl = (int)(kp.nlines - q0 < L ? kp.nlines - q0 : L);
+        const int total = nl * n;
+        const double *src = kp.in + line_base(kp, q0);
+        int l = tid / n, r = tid - (tid / n) * n;
+        const int dl = nthreads / n, dr = nthreads - dl * n;
+        for (int e = tid; e < total; e += nthreads) {
+            copy8_async(sm.tile + (size_t)l * P + r, src + e);
+            l += dl;
+            r += dr;
+            if (r >= n) {
+                r -= n;
+                ++l;
+            }
+        }
+    }
+}
 
 #ifdef __CUDACC__
-template <int RK, bool PER, bool ADJ, int M>
+template <int RK, bool PER, bool ADJ, int M, int IN>
 __device__ __forceinline__ void run_tile(const KParams &kp, const Smem &sm, long long q0)
 {
     Regs<M> R;
     const int tid = threadIdx.x, nthreads = blockDim.x;
 #pragma unroll
     for (int ph = 0; ph < NPHASES; ++ph) {
-        if (!ADJ && (ph == 6 || ph == 7)) continue;
-        tile_phase<RK, PER, ADJ, M>(ph, kp, sm, R, q0, tid, nthreads);
+        if (!phase_used<ADJ, IN>(ph)) continue;
+        tile_phase<RK, PER, ADJ, M, IN>(ph, kp, sm, R, q0, tid, nthreads);
         if (ph + 1 < NPHASES) __syncthreads();
     }
 }
 
 // One CTA = one tile of kp.L lines; blockDim.x >= kp.L * kp.S.
-template <int RK, bool PER, bool ADJ, int M>
-__global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256)) line_kernel(const KParams kp)
+template <int RK, bool PER, bool ADJ, int M, int IN>
+__global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line_kernel(const KParams kp)
 {
     extern __shared__ double smem_raw[];
     const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S);
-    run_tile<RK, PER, ADJ, M>(kp, sm, (long long)blockIdx.x * kp.L);
+    run_tile<RK, PER, ADJ, M, IN>(kp, sm, (long long)blockIdx.x * kp.L);
+}
+
+// Persistent CTAs walk the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// The next tile is copied into the shared tile (cp.async) as soon as the
+// current tile's stencil has read it -- or, for IN_GLOBAL, prefetched into L2
+// -- so the copy overlaps the chains, the backward sweep and the stores.
+template <int RK, bool PER, int M, int IN>
+__global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line_kernel_persist(const KParams kp)
+{
+    extern __shared__ double smem_raw[];
+    using K = LineKernel<RK, PER, false, M, IN>;
+    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S);
+    const int tid = threadIdx.x, nthreads = blockDim.x;
+    const int l = tid % kp.L, s = tid / kp.L;
+    const bool active = s < kp.S;
+    const long long ntiles = (kp.nlines + kp.L - 1) / kp.L;
+    Regs<M> R;
+    long long t = blockIdx.x;
+    if (IN != IN_GLOBAL && t < ntiles) tile_prefetch<IN>(kp, sm, t * kp.L, tid, nthreads);
+    copy_async_commit();
+    for (; t < ntiles; t += gridDim.x) {
+        const long long q0 = t * kp.L;
+        if (IN != IN_GLOBAL) copy_async_wait_all();
+        __syncthreads();
+        if (active) K::fwd(kp, sm, R, l, s, q0);
+        __syncthreads();
+        if (t + gridDim.x < ntiles) tile_prefetch<IN>(kp, sm, (t + gridDim.x) * kp.L, tid, nthreads);
+        copy_async_commit();
+        if (s == 0) K::chain_fwd(kp, sm, l);
+        __syncthreads();
+        if (active) K::bwd(kp, sm, R, l, s);
+        __syncthreads();
+        if (s == 0) K::chain_bwd(kp, sm, l);
+        __syncthreads();
+        if (active) K::template fin<false>(kp, sm, R, l, s, q0);
+    }
 }
 #endif
 
-// Host emulation of one tile (tests): the phases in kernel order over all
-// threads of the CTA.
-template <int RK, bool PER, bool ADJ, int M>
+// Host emulation (tests): the phases in kernel order over all threads of the CTA.
+template <int RK, bool PER, bool ADJ, int M, int IN>
 inline void emulate_tile(const KParams &kp, double *smem, long long q0, int nthreads)
 {
     const Smem sm = carve(smem, kp.L, kp.P, kp.S);
     Regs<M> *R = new Regs<M>[nthreads];
+    if (IN == IN_ROWS)
+        for (int tid = 0; tid < nthreads; ++tid) tile_prefetch<IN_ROWS>(kp, sm, q0, tid, nthreads);
     for (int ph = 0; ph < NPHASES; ++ph) {
-        if (!ADJ && (ph == 6 || ph == 7)) continue;
-        for (int tid = 0; tid < nthreads; ++tid) tile_phase<RK, PER, ADJ, M>(ph, kp, sm, R[tid], q0, tid, nthreads);
+        if (!phase_used<ADJ, IN>(ph)) continue;
+        for (int tid = 0; tid < nthreads; ++tid) tile_phase<RK, PER, ADJ, M, IN>(ph, kp, sm, R[tid], q0, tid, nthreads);
     }
     delete[] R;
 }

@@ -449,6 +449,62 @@ void build_device_table(const Sweep &sw, const Layout &lay, std::vector<double> 
     }
 }
 
+Interior interior_info(const Sweep &sw, const Layout &lay, int m)
+{
+    Interior in;
+    const int nb = sw.nb;
+    if (nb < 16) return in;
+    const int mid = nb / 2;
+    const double ref[7] = {sw.alpha[mid], sw.c1[mid], sw.c2[mid], sw.gamma[mid], sw.d1[mid], sw.d2[mid], sw.delta[mid]};
+    double kmax = 0.0, emax = 0.0;
+    for (int i = 0; i < nb; ++i) {
+        kmax = std::max({kmax, std::fabs(sw.k1[i]), std::fabs(sw.k2[i])});
+        emax = std::max({emax, std::fabs(sw.e1[i]), std::fabs(sw.e2[i])});
+    }
+    // a row is interior when its coefficients equal the line-centre values to
+    // 1e-14 relative (they settle to a few ulps) and its cyclic spike terms
+    // are below 1e-17 of their largest magnitude (their contribution is far
+    // below one rounding of the sums they enter)
+    auto ok = [&](int i) {
+        const double v[7] = {sw.alpha[i], sw.c1[i], sw.c2[i], sw.gamma[i], sw.d1[i], sw.d2[i], sw.delta[i]};
+        for (int k = 0; k < 7; ++k)
+            if (std::fabs(v[k] - ref[k]) > 1e-14 * std::fabs(ref[k])) return false;
+        if (std::fabs(sw.k1[i]) > 1e-17 * kmax || std::fabs(sw.k2[i]) > 1e-17 * kmax) return false;
+        if (std::fabs(sw.e1[i]) > 1e-17 * emax || std::fabs(sw.e2[i]) > 1e-17 * emax) return false;
+        return true;
+    };
+    if (!ok(mid)) return in;
+    int i0 = mid, i1 = mid + 1;
+    while (i0 > 0 && ok(i0 - 1)) --i0;
+    while (i1 < nb && ok(i1)) ++i1;
+    in.i0 = i0;
+    in.i1 = i1;
+    for (int k = 0; k < 7; ++k) in.kc[k] = ref[k];
+    const double c1 = ref[1], c2 = ref[2], d1 = ref[4], d2 = ref[5];
+    // unit responses of a length-m segment under the constant recurrences
+    double z1 = 1.0, z2 = 0.0, y1 = 0.0, y2 = 1.0, zl = 0, zl2 = 0, yl = 0, yl2 = 0;
+    for (int t = 0; t < m; ++t) {
+        const double z = -c1 * z1 - c2 * z2, y = -c1 * y1 - c2 * y2;
+        if (t == m - 2) { zl2 = z; yl2 = y; }
+        if (t == m - 1) { zl = z; yl = y; }
+        z2 = z1; z1 = z; y2 = y1; y1 = y;
+    }
+    double x1 = 1.0, x2 = 0.0, w1 = 0.0, w2 = 1.0, x0 = 0, xs1 = 0, w0 = 0, ws1 = 0;
+    for (int t = m - 1; t >= 0; --t) {
+        const double x = -d1 * x1 - d2 * x2, w = -d1 * w1 - d2 * w2;
+        if (t == 1) { xs1 = x; ws1 = w; }
+        if (t == 0) { x0 = x; w0 = w; }
+        x2 = x1; x1 = x; w2 = w1; w1 = w;
+    }
+    const double pat[8] = {zl, yl, zl2, yl2, x0, w0, xs1, ws1};
+    for (int k = 0; k < 8; ++k) in.pat[k] = pat[k];
+    for (int s = 1; s + 1 < lay.S && s < 32; ++s) {
+        const int a = lay.start(s), len = lay.len(s);
+        if (len == m && a >= i0 && a + len <= i1 && a >= HALO && a + len + HALO <= sw.n) in.mask |= 1u << s;
+    }
+    return in;
+}
+
 std::vector<double> stencil_matrix(const RhsCoef &rc, int n, int bc1, int bcn)
 {
     std::vector<double> B((size_t)n * n, 0.0);
@@ -468,7 +524,7 @@ std::vector<double> stencil_matrix(const RhsCoef &rc, int n, int bc1, int bcn)
         }
         for (int j = 0; j < n; ++j) {
             e[j] = 1.0;
-            B[(size_t)i * n + j] = rhs_closure_row(rc.rk, rc.c, e.data(), n, i, bc1, bcn);
+            B[(size_t)i * n + j] = rhs_closure_row(rc.rk, rc.c, e.data(), 1, n, i, bc1, bcn);
             e[j] = 0.0;
         }
     }

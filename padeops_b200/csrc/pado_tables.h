@@ -47,6 +47,22 @@ Layout make_layout(int n, int m_max);
 // (k1.U, k1.V, k2.U, k2.V).
 void build_device_table(const Sweep &sw, const Layout &lay, std::vector<double> &tab, std::vector<double> &segsum);
 
+// Constant-coefficient interior.  Away from the line ends the factor
+// coefficients of every sweep converge to constants (within ~20-90 rows) and
+// the cyclic spike terms decay to nothing.  Segments that lie wholly in that
+// region, have length m and a full stencil window inside the line run a
+// register-only path: constant coefficients, and the inter-segment
+// corrections computed by the homogeneous recurrence itself.
+struct Interior {
+    unsigned mask = 0;       // bit s: segment s takes the constant-coefficient path
+    double kc[8] = {0};      // alpha, c1, c2, gamma, d1, d2, delta, (unused)
+    // responses of a length-m segment to unit incoming states:
+    // U(m-1), V(m-1), U(m-2), V(m-2), S(0), T(0), S(1), T(1)
+    double pat[8] = {0};
+    int i0 = 0, i1 = 0;      // banded rows treated as interior
+};
+Interior interior_info(const Sweep &sw, const Layout &lay, int m);
+
 // Transposed stencil of a bounded line: B^T rows for the first and last
 // ZB columns.  Dense (n x n) when n <= DENSE_BT_MAX.
 constexpr int BT_ZONE = 8, BT_WIN = 12, DENSE_BT_MAX = 32;

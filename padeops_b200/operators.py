@@ -98,6 +98,10 @@ class _Scheme:
     def set_tiling(self, m: int = 0, lines: int = 0) -> None:
         check(L.lib().pado_set_tiling(self.handle, m, lines), "set_tiling")
 
+    def set_variant(self, variant: int) -> None:
+        """1 = one CTA per tile of lines, 2 = persistent CTAs with prefetch."""
+        check(L.lib().pado_set_kernel_variant(self.handle, variant), "set_variant")
+
     def get_tiling(self) -> tuple[int, int]:
         m, lines = ctypes.c_int(), ctypes.c_int()
         check(L.lib().pado_get_tiling(self.handle, ctypes.byref(m), ctypes.byref(lines)), "get_tiling")

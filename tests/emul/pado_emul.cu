@@ -10,18 +10,26 @@
 
 using namespace pado;
 
+// Every input path the library uses: strided lines through the cp.async
+// rows tile (primal) or straight from global memory (adjoint); contiguous
+// lines through the [L][P] tile.
 template <int RK, bool PER, bool ADJ, int M>
 static void run_all(const KParams &kp, int nthreads)
 {
-    std::vector<double> smem(smem_doubles(kp.L, kp.P, kp.S) + 16, 0.0);
-    for (long long q0 = 0; q0 < kp.nlines; q0 += kp.L) emulate_tile<RK, PER, ADJ, M>(kp, smem.data(), q0, nthreads);
+    const bool strided = kp.stride != 1;
+    const size_t tile = (ADJ || !strided) ? (size_t)kp.L * kp.P : (size_t)kp.n * kp.L;
+    std::vector<double> smem(smem_doubles(kp.L, kp.S, tile), 0.0);
+    for (long long q0 = 0; q0 < kp.nlines; q0 += kp.L) {
+        if (!strided) emulate_tile<RK, PER, ADJ, M, IN_LINES>(kp, smem.data(), q0, nthreads);
+        else if (ADJ) emulate_tile<RK, PER, ADJ, M, IN_GLOBAL>(kp, smem.data(), q0, nthreads);
+        else emulate_tile<RK, PER, ADJ, M, IN_ROWS>(kp, smem.data(), q0, nthreads);
+    }
 }
 
 template <int RK, bool PER, bool ADJ>
 static int pick_m(const KParams &kp, int m, int nthreads)
 {
     switch (m) {
-    case 8: run_all<RK, PER, ADJ, 8>(kp, nthreads); return 0;
     case 16: run_all<RK, PER, ADJ, 16>(kp, nthreads); return 0;
     case 32: run_all<RK, PER, ADJ, 32>(kp, nthreads); return 0;
     case 64: run_all<RK, PER, ADJ, 64>(kp, nthreads); return 0;
@@ -37,7 +45,8 @@ static int pick(const KParams &kp, bool per, bool adj, int m, int nthreads)
 }
 
 extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, int lines,
-                          int extra_threads, int adjoint, int axis, const double *f, double *df, long na, long nb)
+                          int extra_threads, int adjoint, int axis, const double *f, double *df, long na, long nb,
+                          int fast)
 {
     const Sweep prim = primal_sweep(scheme, kind, n, periodic, bc1, bcn);
     const Sweep sw = adjoint ? adjoint_sweep(prim) : prim;
@@ -74,6 +83,10 @@ extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, 
         kp.bt = bt.data();
     }
     kp.rc = rc;
+    const Interior in = interior_info(sw, lay, m);
+    kp.int_mask = fast ? in.mask : 0u;
+    std::memcpy(kp.kc, in.kc, sizeof(kp.kc));
+    std::memcpy(kp.pat, in.pat, sizeof(kp.pat));
     const int nthreads = lines * lay.S + extra_threads;
     switch (rc.rk) {
     case RHS_CD06_D1: return pick<RHS_CD06_D1>(kp, periodic, adjoint, m, nthreads);

@@ -94,23 +94,27 @@ def test_parity_line_lengths(torch_cuda, scheme, kind, n):
                 assert rel_err(got, ref) <= TOL, (axis, periodic, bc1, bcn, rel_err(got, ref))
 
 
-@pytest.mark.parametrize("m,lines", [(8, 8), (8, 32), (16, 16), (32, 8), (32, 16), (64, 8)])
-def test_parity_tilings(torch_cuda, m, lines):
-    """Every segment length / lines-per-CTA the tuner may pick gives the same result."""
+@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("m,lines", [(16, 8), (16, 16), (16, 32), (32, 8), (32, 16), (32, 32), (64, 8)])
+def test_parity_tilings(torch_cuda, m, lines, variant):
+    """Every kernel variant and segment length / lines-per-CTA the tuner may
+    pick gives the oracle's result, along x (tile path) and z (strided paths)."""
     torch = torch_cuda
-    shape = (40, 16, 200)
-    f = spectrum53(shape, seed=5)
-    for scheme, kind in OPS:
-        for periodic in (True, False):
-            op = _make(scheme, 200, 0.05, periodic)
-            try:
-                op.set_tiling(m, lines)
-            except Exception:
-                continue  # not a legal shape for n = 200
-            got = _gpu_apply(torch, op, kind, 1, f, 1 if not periodic else 0, -1 if not periodic else 0)
-            ref = _oracle_apply(scheme, kind, 1, f, 0.05, periodic, 1 if not periodic else 0,
-                                -1 if not periodic else 0)
-            assert rel_err(got, ref) <= TOL
+    n = 256
+    for axis, shape in ((1, (6, 7, n)), (3, (n, 5, 37))):
+        f = spectrum53(shape, seed=5 + axis)
+        for scheme, kind in OPS:
+            for periodic in (True, False):
+                op = _make(scheme, n, 0.05, periodic)
+                op.set_variant(variant)
+                try:
+                    op.set_tiling(m, lines)
+                except Exception:
+                    continue  # not a legal shape for this n
+                bc = (0, 0) if periodic else (1, -1)
+                got = _gpu_apply(torch, op, kind, axis, f, *bc)
+                ref = _oracle_apply(scheme, kind, axis, f, 0.05, periodic, *bc)
+                assert rel_err(got, ref) <= TOL, (axis, scheme, kind, periodic, rel_err(got, ref))
 
 
 def test_config1_cd06_64cube(torch_cuda):
