@@ -127,12 +127,22 @@ int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, doub
  * (8/16/32).  0 keeps the current value.  Rebuilds the handle's tables. */
 int pado_set_tiling(pado_op_t op, int m, int lines);
 int pado_get_tiling(pado_op_t op, int *m, int *lines);
-/* Kernel organisation of the forward operator: 1 = one CTA per tile of
- * lines (the default, 0 selects it), 2 = persistent CTAs that prefetch the
- * next tile with cp.async while the current one is solved, 3 = persistent
- * CTAs that read lines straight into registers and warm L2 with the next
- * tile (strided axes; x lines use 2). */
+/* Kernel organisation of the forward operator: 0 = automatic (the
+ * streaming kernel where the field allows it, else 1; the default),
+ * 1 = one CTA per tile of lines, 2 = persistent CTAs that prefetch the next
+ * tile with cp.async while the current one is solved, 3 = persistent CTAs
+ * that read lines straight into registers and warm L2 with the next tile
+ * (strided axes; x lines use 2), 4 = the streaming kernel: persistent CTAs
+ * fed by TMA tensor / bulk copies two tiles ahead (needs 16-byte aligned
+ * fields, an even x extent for y/z lines and an even n for x lines;
+ * PADO_E_UNSUPPORTED otherwise).  Adjoints always use 1.
+ * No counterpart in the reference (a B200 tuning knob). */
 int pado_set_kernel_variant(pado_op_t op, int variant);
+/* Device-side status of the handle's kernels: PADO_OK, or PADO_E_TIMEOUT
+ * when a streaming kernel's bounded wait for its copies expired (its CTAs
+ * then stop early and the output is incomplete).  Synchronous (reads device
+ * memory); clear != 0 resets the word.  No counterpart in the reference. */
+int pado_device_status(pado_op_t op, int clear);
 
 /* ---- batched execution (many fields, one persistent launch) ------------ */
 

@@ -1,5 +1,6 @@
 // pado_api.cu -- the C ABI of include/pado.h: scheme objects, table upload,
 // kernel dispatch and the host-buffer path.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -19,6 +20,7 @@ using namespace pado;
 
 namespace pado {
 std::atomic<long long> g_launches{0};
+static_assert(PADO_STATUS_TIMEOUT == PADO_E_TIMEOUT, "device and host timeout codes differ");
 }
 
 namespace pado {
@@ -44,22 +46,6 @@ namespace {
 
 int max_threads_for_m(int m) { return m >= 64 ? 256 : 512; }
 
-int upload(pado_op_s *op, const std::vector<double> &h, double **d)
-{
-    if (h.empty()) {
-        *d = nullptr;
-        return PADO_OK;
-    }
-    void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, h.size() * sizeof(double));
-    if (e != cudaSuccess) return cuda_fail(e);
-    op->allocations.push_back(p);
-    e = cudaMemcpy(p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_fail(e);
-    *d = static_cast<double *>(p);
-    return PADO_OK;
-}
-
 // Default tiling: segment length and lines per CTA for a line of length n.
 void default_tiling(int n, int *m, int *lines)
 {
@@ -68,6 +54,21 @@ void default_tiling(int n, int *m, int *lines)
     int L = 32;
     while (L > 8 && L * S > max_threads_for_m(*m)) L /= 2;
     *lines = L;
+}
+
+template <typename T>
+int upload_vec(pado_op_s *op, const std::vector<T> &h, T **d)
+{
+    *d = nullptr;
+    if (h.empty()) return PADO_OK;
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, h.size() * sizeof(T));
+    if (e != cudaSuccess) return cuda_fail(e);
+    op->allocations.push_back(p);
+    e = cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e);
+    *d = static_cast<T *>(p);
+    return PADO_OK;
 }
 
 int build_tables(pado_op_s *op)
@@ -89,34 +90,18 @@ int build_tables(pado_op_s *op)
         for (auto [b1, bn] : bcs) {
             // cd06 takes its closures from init (cd06.F90:177)
             const int cb1 = op->scheme == CD06 ? op->bc1 : b1, cbn = op->scheme == CD06 ? op->bcn : bn;
-            const Sweep prim = primal_sweep(op->scheme, kind, n, op->periodic, cb1, cbn);
-            const Sweep adj = adjoint_sweep(prim);
-            const RhsCoef rc = make_rhs_coef(op->scheme, kind, op->dx, op->periodic);
-            const Layout lay = make_layout(n, op->m);
             for (int dir = 0; dir < 2; ++dir) {
-                const Sweep &sw = dir == 0 ? prim : adj;
                 DevTables dt;
-                dt.nb = sw.nb;
-                dt.nbord = sw.nbord;
-                dt.lay = lay;
-                dt.rc = rc;
-                std::memcpy(dt.mb, sw.mb, sizeof(dt.mb));
-                std::vector<double> tab, segsum;
-                build_device_table(sw, lay, tab, segsum);
-                dt.interior = interior_info(sw, lay, op->m);
-                int rc_ = upload(op, tab, &dt.tab);
-                if (rc_ == PADO_OK) rc_ = upload(op, segsum, &dt.segsum);
-                if (rc_ != PADO_OK) return rc_;
-                if (dir == 1) {
-                    double taps[9];
-                    interior_taps(rc, taps);
-                    for (int k = 0; k < 9; ++k) dt.taps[k] = taps[8 - k];  // B^T: tap at offset o is c_{-o}
-                    if (!op->periodic) {
-                        rc_ = upload(op, transposed_stencil_blocks(rc, n, cb1, cbn), &dt.bt);
-                        if (rc_ != PADO_OK) return rc_;
-                    }
-                }
-                op->tables[TabKey(kind, b1, bn, dir)] = dt;
+                dt.host = make_op_tables(op->scheme, kind, n, op->dx, op->periodic, cb1, cbn, op->m, dir == 1);
+                const OpTables &h = dt.host;
+                int rc = upload_vec(op, h.tab, &dt.tab);
+                if (rc == PADO_OK) rc = upload_vec(op, h.ctab, &dt.ctab);
+                if (rc == PADO_OK) rc = upload_vec(op, h.ctab_exact, &dt.ctab_exact);
+                if (rc == PADO_OK) rc = upload_vec(op, h.etab, &dt.etab);
+                if (rc == PADO_OK) rc = upload_vec(op, h.toff, &dt.toff);
+                if (rc == PADO_OK) rc = upload_vec(op, h.bt, &dt.bt);
+                if (rc != PADO_OK) return rc;
+                op->tables[TabKey(kind, b1, bn, dir)] = std::move(dt);
             }
         }
     }
@@ -133,29 +118,144 @@ KernelFn pick_kernel(int rk, bool per, bool adj, bool contiguous, int m, int var
     }
 }
 
-// Geometry of the line family for (axis, na, nb).
-void set_geometry(KParams &kp, int axis, int n, long long na, long long nb)
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link
+// against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled()
 {
-    kp.nlines = na * nb;
-    if (axis == 1) {
-        kp.line_ia = 1;
-        kp.line_oc = n;
-        kp.stride = 1;
-    } else if (axis == 2) {
-        kp.line_ia = na;
-        kp.line_oc = na * (long long)n;
-        kp.stride = na;
-    } else {
-        kp.line_ia = kp.nlines > 0 ? kp.nlines : 1;
-        kp.line_oc = 0;
-        kp.stride = na * nb;
+    static EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            (void)cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+StreamFn pick_stream(int rk, bool per, int m, bool xl)
+{
+    switch (rk) {
+    case RHS_CD06_D1: return pick_stream_rk0(per, m, xl);
+    case RHS_CD10_D1: return pick_stream_rk1(per, m, xl);
+    case RHS_CD10_D2: return pick_stream_rk2(per, m, xl);
+    default: return pick_stream_rk3(per, m, xl);
     }
+}
+
+int round16(long long v) { return (int)((v + 15) / 16 * 16); }
+
+// Plan of a streaming launch (primal): lines per tile, stages, shared memory
+// and the copy descriptors.  False when the field or tiling does not fit it
+// (odd strides, unaligned pointers, a table too large to stage); the caller
+// then runs the one-CTA-per-tile kernel.
+bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, int axis, long long na, long long nb,
+                 StreamParams *sp, int *threads, size_t *smem)
+{
+    const int n = op->n, S = kp0.S;
+    if (op->m != 16 && op->m != 32 && op->m != 64) return false;
+    const bool xl = axis == 1;
+    const size_t align_bits = reinterpret_cast<size_t>(kp0.in) | reinterpret_cast<size_t>(kp0.out);
+    if (align_bits & 15) return false;
+    if (xl ? (n % 2 != 0) : (na % 2 != 0 || na > 0x7fffffffLL || nb > 0x7fffffffLL)) return false;
+    const int etab_rows = (int)(dt.host.etab.size() / T_NF);
+    for (int L : {32, 16, 8}) {
+        if (L * S > 256) continue;
+        for (int stages : {2, 1}) {
+            int P = kp0.P, box_rows = 0, nbox = 0, tile_doubles;
+            if (xl) {
+                P = n + 2;  // rows 16-byte aligned for the bulk copies
+                tile_doubles = round16((long long)L * P);
+            } else {
+                // boxes of at most 256 rows; a multiple of 16 rows keeps every
+                // box's shared-memory destination 128-byte aligned for any L
+                nbox = (n + 255) / 256;
+                box_rows = ((n + nbox - 1) / nbox + 15) / 16 * 16;
+                tile_doubles = round16((long long)nbox * box_rows * L);
+            }
+            const size_t bytes = stream_smem_bytes(L, S, stages, tile_doubles, etab_rows);
+            if (bytes > 227 * 1024) continue;
+            std::memset(sp, 0, sizeof(*sp));
+            sp->kp = kp0;
+            sp->kp.L = L;
+            sp->kp.P = P;
+            sp->axis = axis;
+            sp->stages = stages;
+            sp->box_rows = box_rows;
+            sp->nbox = nbox;
+            sp->tile_doubles = tile_doubles;
+            sp->etab_rows = etab_rows;
+            sp->etab = dt.etab;
+            sp->toff = dt.toff;
+            sp->status = op->d_status;
+            if (xl) {
+                sp->ntiles = (kp0.nlines + L - 1) / L;
+            } else {
+                sp->na = (int)na;
+                sp->xblocks = (int)((na + L - 1) / L);
+                sp->ntiles = (long long)sp->xblocks * nb;
+                sp->pstride = axis == 2 ? na * (long long)n : na;
+                EncodeTiledFn enc = encode_tiled();
+                if (!enc) return false;
+                const cuuint64_t dims[3] = {(cuuint64_t)na, (cuuint64_t)(axis == 2 ? n : nb),
+                                            (cuuint64_t)(axis == 2 ? nb : n)};
+                const cuuint64_t strides[2] = {(cuuint64_t)na * 8, (cuuint64_t)na * (axis == 2 ? n : nb) * 8};
+                const cuuint32_t box[3] = {(cuuint32_t)L, (cuuint32_t)(axis == 2 ? box_rows : 1),
+                                           (cuuint32_t)(axis == 2 ? 1 : box_rows)};
+                const cuuint32_t estr[3] = {1, 1, 1};
+                if (enc(&sp->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(kp0.in), dims, strides, box,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                    return false;
+            }
+            *threads = L * S;
+            *smem = bytes;
+            return true;
+        }
+    }
+    return false;
+}
+
+int sm_count()
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+
+int launch_stream(pado_op_s *op, const StreamParams &sp, int threads, size_t smem, cudaStream_t st)
+{
+    StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1);
+    {
+        static std::mutex attr_mu;
+        static std::map<const void *, size_t> granted;
+        std::lock_guard<std::mutex> g(attr_mu);
+        size_t &have = granted[(const void *)fn];
+        if (have < smem) {
+            cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return cuda_fail(e);
+            have = smem;
+        }
+    }
+    const long long grid = std::min<long long>(sp.ntiles, sm_count());
+    if (grid < 1) return PADO_OK;
+    fn<<<(unsigned)grid, threads, smem, st>>>(sp);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PADO_OK : cuda_fail(e);
 }
 
 }  // namespace
 
 int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
-                         int bcn, bool adjoint, int lines, KParams *kpo, bool *trivial)
+                         int bcn, bool adjoint, int lines, bool no_fast, KParams *kpo, bool *trivial)
 {
     *trivial = true;
     if (!op) return PADO_E_NULL;
@@ -176,28 +276,19 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
     const DevTables &dt = it->second;
 
     KParams kp{};
+    fill_params(kp, dt.host, n, op->scheme == CD06 ? op->bc1 : bc1, op->scheme == CD06 ? op->bcn : bcn);
     kp.in = f;
     kp.out = df;
     set_geometry(kp, axis, n, na, nb);
-    kp.n = n;
-    kp.nb = dt.nb;
-    kp.nbord = dt.nbord;
-    kp.P = (n % 2 == 0) ? n + 1 : n;
-    kp.S = dt.lay.S;
-    kp.base = dt.lay.base;
-    kp.rem = dt.lay.rem;
     kp.L = lines;
-    kp.bc1 = op->scheme == CD06 ? op->bc1 : bc1;
-    kp.bcn = op->scheme == CD06 ? op->bcn : bcn;
     kp.tab = dt.tab;
-    kp.segsum = dt.segsum;
+    kp.ctab = dt.ctab;
     kp.bt = dt.bt;
-    std::memcpy(kp.mb, dt.mb, sizeof(kp.mb));
-    std::memcpy(kp.taps, dt.taps, sizeof(kp.taps));
-    kp.rc = dt.rc;
-    kp.int_mask = dt.interior.mask;
-    std::memcpy(kp.kc, dt.interior.kc, sizeof(kp.kc));
-    std::memcpy(kp.pat, dt.interior.pat, sizeof(kp.pat));
+    if (no_fast) {
+        // every segment on the per-row table (kernels built for another segment length)
+        kp.int_mask = 0;
+        kp.ctab = dt.ctab_exact;
+    }
     *kpo = kp;
     *trivial = false;
     return PADO_OK;
@@ -210,7 +301,7 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
 {
     KParams kp;
     bool trivial = true;
-    int rc = prepare_launch(op, kind, axis, f, df, na, nb, bc1, bcn, adjoint, op ? op->lines : 0, &kp, &trivial);
+    int rc = prepare_launch(op, kind, axis, f, df, na, nb, bc1, bcn, adjoint, op ? op->lines : 0, false, &kp, &trivial);
     if (rc != PADO_OK) return rc;
     if (trivial) {
         const long long total = (long long)op->n * na * nb;
@@ -219,6 +310,16 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
         cudaError_t e = (kind == FILTER) ? cudaMemcpyAsync(df, f, total * sizeof(double), cudaMemcpyDeviceToDevice, st)
                                          : cudaMemsetAsync(df, 0, total * sizeof(double), st);
         return e == cudaSuccess ? PADO_OK : cuda_fail(e);
+    }
+    if (!adjoint && (op->variant == 0 || op->variant == 4)) {
+        const bool bounded_bc = !op->periodic && op->scheme != CD06;
+        const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, 0));
+        StreamParams sp;
+        int sthreads = 0;
+        size_t ssmem = 0;
+        if (plan_stream(op, dt, kp, axis, na, nb, &sp, &sthreads, &ssmem))
+            return launch_stream(op, sp, sthreads, ssmem, st);
+        if (op->variant == 4) return PADO_E_UNSUPPORTED;
     }
     const int threads = kp.L * kp.S;
     if (threads > max_threads_for_m(op->m)) return PADO_E_SIZE;
@@ -282,6 +383,15 @@ int pado_create(pado_op_t *out, int scheme, int n, double dx, int periodic, int 
     op->bcn = bcn;
     cudaGetDevice(&op->device);
     default_tiling(n, &op->m, &op->lines);
+    {
+        cudaError_t e = cudaMalloc(&op->d_status, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemset(op->d_status, 0, sizeof(int));
+        if (e != cudaSuccess) {
+            const int rc = cuda_fail(e);
+            pado_destroy(op);
+            return rc;
+        }
+    }
     int rc = build_tables(op);
     if (rc != PADO_OK) {
         pado_destroy(op);
@@ -307,6 +417,7 @@ void pado_destroy(pado_op_t op)
     for (void *p : op->allocations) cudaFree(p);
     if (op->stage_f) cudaFree(op->stage_f);
     if (op->stage_df) cudaFree(op->stage_df);
+    if (op->d_status) cudaFree(op->d_status);
     delete op;
 }
 
@@ -390,9 +501,24 @@ int pado_set_tiling(pado_op_t op, int m, int lines)
 int pado_set_kernel_variant(pado_op_t op, int variant)
 {
     if (!op) return PADO_E_NULL;
-    if (variant < 0 || variant > 3) return PADO_E_ARG;
-    op->variant = variant == 0 ? 1 : variant;
+    if (variant < 0 || variant > 4) return PADO_E_ARG;
+    op->variant = variant;
     return PADO_OK;
+}
+
+int pado_device_status(pado_op_t op, int clear)
+{
+    if (!op) return PADO_E_NULL;
+    if (!op->d_status) return PADO_OK;
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, op->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (clear && v != 0) {
+        const int zero = 0;
+        e = cudaMemcpy(op->d_status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e);
+    }
+    return v;
 }
 
 int pado_get_tiling(pado_op_t op, int *m, int *lines)

@@ -52,14 +52,14 @@ int layout_items(pado_batch_s *b)
         if (L < 1) return PADO_E_SIZE;
         KParams kp;
         bool trivial = true;
-        int rc = prepare_launch(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, false, L, &kp,
-                                &trivial);
+        // the register-only path assumes segments of BATCH_M rows
+        int rc = prepare_launch(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, false, L,
+                                it.op->m != BATCH_M, &kp, &trivial);
         if (rc != PADO_OK) return rc;
         if (trivial) {
             if (it.op->n == 1 && (long long)na * nb > 0) return PADO_E_UNSUPPORTED;  // n == 1 items: use pado_apply
             continue;
         }
-        if (it.op->m != BATCH_M) kp.int_mask = 0;  // the register-only path assumes segments of BATCH_M rows
         Pre p{};
         p.d.kp = kp;
         p.d.code = kp.rc.rk * 4 + (it.op->periodic ? 2 : 0) + (kp.stride != 1 ? 1 : 0);

@@ -128,24 +128,52 @@ struct Cf90Const {
 };
 
 // ---------------------------------------------------------------------------
+// A double whose products and sums round one at a time (no fused
+// multiply-add).  The stencils below evaluate with it so that their
+// cancelling sums round exactly like the reference's expressions: one-sided
+// closures add terms of size f/dx whose sum is orders of magnitude smaller,
+// and a contracted product there moves the result by more than the parity
+// bar.  The recurrences of the solve are well conditioned and keep FMA.
+// ---------------------------------------------------------------------------
+struct NC {
+    double v;
+    PADO_HD PADO_INLINE explicit NC(double x) : v(x) {}
+};
+#ifdef __CUDA_ARCH__
+PADO_HD PADO_INLINE NC operator*(NC a, NC b) { return NC(__dmul_rn(a.v, b.v)); }
+PADO_HD PADO_INLINE NC operator+(NC a, NC b) { return NC(__dadd_rn(a.v, b.v)); }
+PADO_HD PADO_INLINE NC operator-(NC a, NC b) { return NC(__dsub_rn(a.v, b.v)); }
+#else
+PADO_HD PADO_INLINE NC operator*(NC a, NC b) { return NC(a.v * b.v); }
+PADO_HD PADO_INLINE NC operator+(NC a, NC b) { return NC(a.v + b.v); }
+PADO_HD PADO_INLINE NC operator-(NC a, NC b) { return NC(a.v - b.v); }
+#endif
+PADO_HD PADO_INLINE NC operator-(NC a) { return NC(-a.v); }
+PADO_HD PADO_INLINE NC operator*(double a, NC b) { return NC(a) * b; }
+
+// ---------------------------------------------------------------------------
 // Interior stencils on a 9-point window v[0..8] = f(i-4..i+4).
 // ---------------------------------------------------------------------------
-PADO_HD PADO_INLINE double rhs_interior(int rk, int periodic, const double *c, const double *v)
+PADO_HD PADO_INLINE double rhs_interior(int rk, int periodic, const double *cc, const double *vv)
 {
+#define c(k) NC(cc[k])
+#define v(k) NC(vv[k])
     switch (rk) {
     case RHS_CD06_D1:
         // periodic: cd06.F90:541-542; bounded rows 4..n-3: cd06.F90:575-576 (b term first)
-        if (periodic) return c[0] * (v[5] - v[3]) + c[1] * (v[6] - v[2]);
-        return c[1] * (v[6] - v[2]) + c[0] * (v[5] - v[3]);
+        if (periodic) return (c(0) * (v(5) - v(3)) + c(1) * (v(6) - v(2))).v;
+        return (c(1) * (v(6) - v(2)) + c(0) * (v(5) - v(3))).v;
     case RHS_CD10_D1:  // cd10.F90:1129-1131, 1209-1211
-        return c[0] * (v[5] - v[3]) + c[1] * (v[6] - v[2]) + c[2] * (v[7] - v[1]);
+        return (c(0) * (v(5) - v(3)) + c(1) * (v(6) - v(2)) + c(2) * (v(7) - v(1))).v;
     case RHS_CD10_D2:  // cd10.F90:1619-1621, 1692-1694
-        return c[0] * (v[5] - 2.0 * v[4] + v[3]) + c[1] * (v[6] - 2.0 * v[4] + v[2]) +
-               c[2] * (v[7] - 2.0 * v[4] + v[1]);
+        return (c(0) * (v(5) - 2.0 * v(4) + v(3)) + c(1) * (v(6) - 2.0 * v(4) + v(2)) +
+                c(2) * (v(7) - 2.0 * v(4) + v(1))).v;
     default:  // cf90.F90:643-647, 735-739
-        return c[0] * (v[4]) + c[1] * (v[5] + v[3]) + c[2] * (v[6] + v[2]) + c[3] * (v[7] + v[1]) +
-               c[4] * (v[8] + v[0]);
+        return (c(0) * (v(4)) + c(1) * (v(5) + v(3)) + c(2) * (v(6) + v(2)) + c(3) * (v(7) + v(1)) +
+                c(4) * (v(8) + v(0))).v;
     }
+#undef c
+#undef v
 }
 
 // ---------------------------------------------------------------------------
@@ -157,133 +185,131 @@ PADO_HD PADO_INLINE double rhs_interior(int rk, int periodic, const double *c, c
 PADO_HD inline double rhs_closure_row(int rk, const double *c, const double *line, long long stride, int n, int row,
                                       int bc1, int bcn)
 {
-#define F(j) line[(long long)((j)-1) * stride]
+#define F(j) NC(line[(long long)((j)-1) * stride])
     const int i = row + 1;  // 1-based
     const bool left = i <= closure_rows(rk);
     switch (rk) {
     case RHS_CD06_D1: {
         // cd06.F90:565-585 (bc is fixed at init; only bc=0 closures exist)
-        const double a_np_1 = c[2], b_np_1 = c[3], c_np_1 = c[4], d_np_1 = c[5], a_np_2 = c[6], a_np_3 = c[7],
-                     b_np_3 = c[8];
-        if (i == 1) return a_np_1 * F(1) + b_np_1 * F(2) + c_np_1 * F(3) + d_np_1 * F(4);
-        if (i == 2) return a_np_2 * (F(3) - F(1));
-        if (i == 3) return a_np_3 * (F(4) - F(2)) + b_np_3 * (F(5) - F(1));
-        if (i == n - 2) return a_np_3 * (F(n - 1) - F(n - 3)) + b_np_3 * (F(n) - F(n - 4));
-        if (i == n - 1) return a_np_2 * (F(n) - F(n - 2));
-        return -(a_np_1 * F(n)) - b_np_1 * F(n - 1) - c_np_1 * F(n - 2) - d_np_1 * F(n - 3);
+        const NC a_np_1(c[2]), b_np_1(c[3]), c_np_1(c[4]), d_np_1(c[5]), a_np_2(c[6]), a_np_3(c[7]), b_np_3(c[8]);
+        if (i == 1) return (a_np_1 * F(1) + b_np_1 * F(2) + c_np_1 * F(3) + d_np_1 * F(4)).v;
+        if (i == 2) return (a_np_2 * (F(3) - F(1))).v;
+        if (i == 3) return (a_np_3 * (F(4) - F(2)) + b_np_3 * (F(5) - F(1))).v;
+        if (i == n - 2) return (a_np_3 * (F(n - 1) - F(n - 3)) + b_np_3 * (F(n) - F(n - 4))).v;
+        if (i == n - 1) return (a_np_2 * (F(n) - F(n - 2))).v;
+        return (-(a_np_1 * F(n)) - b_np_1 * F(n - 1) - c_np_1 * F(n - 2) - d_np_1 * F(n - 3)).v;
     }
     case RHS_CD10_D1: {
         // cd10.F90:1164-1258
-        const double a10 = c[0], b10 = c[1], c10 = c[2], a_np_4 = c[3], b_np_4 = c[4], c_np_4 = c[5],
-                     a_np_3 = c[6], b_np_3 = c[7], a_np_2 = c[8], a_np_1 = c[9], b_np_1 = c[10], c_np_1 = c[11],
-                     d_np_1 = c[12];
+        const NC a10(c[0]), b10(c[1]), c10(c[2]), a_np_4(c[3]), b_np_4(c[4]), c_np_4(c[5]), a_np_3(c[6]),
+                         b_np_3(c[7]), a_np_2(c[8]), a_np_1(c[9]), b_np_1(c[10]), c_np_1(c[11]), d_np_1(c[12]);
         if (left) {
             if (bc1 == 0) {
-                if (i == 1) return a_np_1 * F(1) + b_np_1 * F(2) + c_np_1 * F(3) + d_np_1 * F(4);
-                if (i == 2) return a_np_2 * (F(3) - F(1));
-                if (i == 3) return a_np_3 * (F(4) - F(2)) + b_np_3 * (F(5) - F(1));
-                return a_np_4 * (F(5) - F(3)) + b_np_4 * (F(6) - F(2)) + c_np_4 * (F(7) - F(1));
+                if (i == 1) return (a_np_1 * F(1) + b_np_1 * F(2) + c_np_1 * F(3) + d_np_1 * F(4)).v;
+                if (i == 2) return (a_np_2 * (F(3) - F(1))).v;
+                if (i == 3) return (a_np_3 * (F(4) - F(2)) + b_np_3 * (F(5) - F(1))).v;
+                return (a_np_4 * (F(5) - F(3)) + b_np_4 * (F(6) - F(2)) + c_np_4 * (F(7) - F(1))).v;
             }
             if (bc1 == 1) {
                 if (i == 1) return 0.0;
-                if (i == 2) return a10 * (F(3) - F(1)) + b10 * (F(4) - F(2)) + c10 * (F(5) - F(3));
-                if (i == 3) return a10 * (F(4) - F(2)) + b10 * (F(5) - F(1)) + c10 * (F(6) - F(2));
-                return a10 * (F(5) - F(3)) + b10 * (F(6) - F(2)) + c10 * (F(7) - F(1));
+                if (i == 2) return (a10 * (F(3) - F(1)) + b10 * (F(4) - F(2)) + c10 * (F(5) - F(3))).v;
+                if (i == 3) return (a10 * (F(4) - F(2)) + b10 * (F(5) - F(1)) + c10 * (F(6) - F(2))).v;
+                return (a10 * (F(5) - F(3)) + b10 * (F(6) - F(2)) + c10 * (F(7) - F(1))).v;
             }
-            if (i == 1) return a10 * (F(2) + F(2)) + b10 * (F(3) + F(3)) + c10 * (F(4) + F(4));
-            if (i == 2) return a10 * (F(3) - F(1)) + b10 * (F(4) + F(2)) + c10 * (F(5) + F(3));
-            if (i == 3) return a10 * (F(4) - F(2)) + b10 * (F(5) - F(1)) + c10 * (F(6) + F(2));
-            return a10 * (F(5) - F(3)) + b10 * (F(6) - F(2)) + c10 * (F(7) - F(1));
+            if (i == 1) return (a10 * (F(2) + F(2)) + b10 * (F(3) + F(3)) + c10 * (F(4) + F(4))).v;
+            if (i == 2) return (a10 * (F(3) - F(1)) + b10 * (F(4) + F(2)) + c10 * (F(5) + F(3))).v;
+            if (i == 3) return (a10 * (F(4) - F(2)) + b10 * (F(5) - F(1)) + c10 * (F(6) + F(2))).v;
+            return (a10 * (F(5) - F(3)) + b10 * (F(6) - F(2)) + c10 * (F(7) - F(1))).v;
         }
         if (bcn == 0) {
-            if (i == n - 3) return a_np_4 * (F(n - 2) - F(n - 4)) + b_np_4 * (F(n - 1) - F(n - 5)) + c_np_4 * (F(n) - F(n - 6));
-            if (i == n - 2) return a_np_3 * (F(n - 1) - F(n - 3)) + b_np_3 * (F(n) - F(n - 4));
-            if (i == n - 1) return a_np_2 * (F(n) - F(n - 2));
-            return -(a_np_1 * F(n)) - b_np_1 * F(n - 1) - c_np_1 * F(n - 2) - d_np_1 * F(n - 3);
+            if (i == n - 3) return (a_np_4 * (F(n - 2) - F(n - 4)) + b_np_4 * (F(n - 1) - F(n - 5)) + c_np_4 * (F(n) - F(n - 6))).v;
+            if (i == n - 2) return (a_np_3 * (F(n - 1) - F(n - 3)) + b_np_3 * (F(n) - F(n - 4))).v;
+            if (i == n - 1) return (a_np_2 * (F(n) - F(n - 2))).v;
+            return (-(a_np_1 * F(n)) - b_np_1 * F(n - 1) - c_np_1 * F(n - 2) - d_np_1 * F(n - 3)).v;
         }
         if (bcn == 1) {
-            if (i == n - 3) return a10 * (F(n - 2) - F(n - 4)) + b10 * (F(n - 1) - F(n - 5)) + c10 * (F(n) - F(n - 6));
-            if (i == n - 2) return a10 * (F(n - 1) - F(n - 3)) + b10 * (F(n) - F(n - 4)) + c10 * (F(n - 1) - F(n - 5));
-            if (i == n - 1) return a10 * (F(n) - F(n - 2)) + b10 * (F(n - 1) - F(n - 3)) + c10 * (F(n - 2) - F(n - 4));
+            if (i == n - 3) return (a10 * (F(n - 2) - F(n - 4)) + b10 * (F(n - 1) - F(n - 5)) + c10 * (F(n) - F(n - 6))).v;
+            if (i == n - 2) return (a10 * (F(n - 1) - F(n - 3)) + b10 * (F(n) - F(n - 4)) + c10 * (F(n - 1) - F(n - 5))).v;
+            if (i == n - 1) return (a10 * (F(n) - F(n - 2)) + b10 * (F(n - 1) - F(n - 3)) + c10 * (F(n - 2) - F(n - 4))).v;
             return 0.0;
         }
-        if (i == n - 3) return a10 * (F(n - 2) - F(n - 4)) + b10 * (F(n - 1) - F(n - 5)) + c10 * (F(n) - F(n - 6));
-        if (i == n - 2) return a10 * (F(n - 1) - F(n - 3)) + b10 * (F(n) - F(n - 4)) + c10 * (-F(n - 1) - F(n - 5));
-        if (i == n - 1) return a10 * (F(n) - F(n - 2)) + b10 * (-F(n - 1) - F(n - 3)) + c10 * (-F(n - 2) - F(n - 4));
-        return a10 * (-F(n - 1) - F(n - 1)) + b10 * (-F(n - 2) - F(n - 2)) + c10 * (-F(n - 3) - F(n - 3));
+        if (i == n - 3) return (a10 * (F(n - 2) - F(n - 4)) + b10 * (F(n - 1) - F(n - 5)) + c10 * (F(n) - F(n - 6))).v;
+        if (i == n - 2) return (a10 * (F(n - 1) - F(n - 3)) + b10 * (F(n) - F(n - 4)) + c10 * (-F(n - 1) - F(n - 5))).v;
+        if (i == n - 1) return (a10 * (F(n) - F(n - 2)) + b10 * (-F(n - 1) - F(n - 3)) + c10 * (-F(n - 2) - F(n - 4))).v;
+        return (a10 * (-F(n - 1) - F(n - 1)) + b10 * (-F(n - 2) - F(n - 2)) + c10 * (-F(n - 3) - F(n - 3))).v;
     }
     case RHS_CD10_D2: {
         // cd10.F90:1654-1730
-        const double a10 = c[0], b10 = c[1], c10 = c[2], a_np_3 = c[3], b_np_3 = c[4], a_np_2 = c[5],
-                     a_np_1 = c[6], b_np_1 = c[7], c_np_1 = c[8], d_np_1 = c[9], e_np_1 = c[10];
+        const NC a10(c[0]), b10(c[1]), c10(c[2]), a_np_3(c[3]), b_np_3(c[4]), a_np_2(c[5]), a_np_1(c[6]),
+                         b_np_1(c[7]), c_np_1(c[8]), d_np_1(c[9]), e_np_1(c[10]);
         if (left) {
             if (bc1 == 0) {
-                if (i == 1) return a_np_1 * F(1) + b_np_1 * F(2) + c_np_1 * F(3) + d_np_1 * F(4) + e_np_1 * F(5);
-                if (i == 2) return a_np_2 * (F(3) - 2.0 * F(2) + F(1));
-                return a_np_3 * (F(4) - 2.0 * F(3) + F(2)) + b_np_3 * (F(5) - 2.0 * F(3) + F(1));
+                if (i == 1) return (a_np_1 * F(1) + b_np_1 * F(2) + c_np_1 * F(3) + d_np_1 * F(4) + e_np_1 * F(5)).v;
+                if (i == 2) return (a_np_2 * (F(3) - 2.0 * F(2) + F(1))).v;
+                return (a_np_3 * (F(4) - 2.0 * F(3) + F(2)) + b_np_3 * (F(5) - 2.0 * F(3) + F(1))).v;
             }
             if (bc1 == 1) {
-                if (i == 1) return a10 * (F(2) - 2.0 * F(1) + F(2)) + b10 * (F(3) - 2.0 * F(1) + F(3)) + c10 * (F(4) - 2.0 * F(1) + F(4));
-                if (i == 2) return a10 * (F(3) - 2.0 * F(2) + F(1)) + b10 * (F(4) - 2.0 * F(2) + F(2)) + c10 * (F(5) - 2.0 * F(2) + F(3));
-                return a10 * (F(4) - 2.0 * F(3) + F(2)) + b10 * (F(5) - 2.0 * F(3) + F(1)) + c10 * (F(6) - 2.0 * F(3) + F(2));
+                if (i == 1) return (a10 * (F(2) - 2.0 * F(1) + F(2)) + b10 * (F(3) - 2.0 * F(1) + F(3)) + c10 * (F(4) - 2.0 * F(1) + F(4))).v;
+                if (i == 2) return (a10 * (F(3) - 2.0 * F(2) + F(1)) + b10 * (F(4) - 2.0 * F(2) + F(2)) + c10 * (F(5) - 2.0 * F(2) + F(3))).v;
+                return (a10 * (F(4) - 2.0 * F(3) + F(2)) + b10 * (F(5) - 2.0 * F(3) + F(1)) + c10 * (F(6) - 2.0 * F(3) + F(2))).v;
             }
-            if (i == 1) return a10 * (F(2) - 2.0 * F(1) - F(2)) + b10 * (F(3) - 2.0 * F(1) - F(3)) + c10 * (F(4) - 2.0 * F(1) - F(4));
-            if (i == 2) return a10 * (F(3) - 2.0 * F(2) + F(1)) + b10 * (F(4) - 2.0 * F(2) - F(2)) + c10 * (F(5) - 2.0 * F(2) - F(3));
-            return a10 * (F(4) - 2.0 * F(3) + F(2)) + b10 * (F(5) - 2.0 * F(3) + F(1)) + c10 * (F(6) - 2.0 * F(3) - F(2));
+            if (i == 1) return (a10 * (F(2) - 2.0 * F(1) - F(2)) + b10 * (F(3) - 2.0 * F(1) - F(3)) + c10 * (F(4) - 2.0 * F(1) - F(4))).v;
+            if (i == 2) return (a10 * (F(3) - 2.0 * F(2) + F(1)) + b10 * (F(4) - 2.0 * F(2) - F(2)) + c10 * (F(5) - 2.0 * F(2) - F(3))).v;
+            return (a10 * (F(4) - 2.0 * F(3) + F(2)) + b10 * (F(5) - 2.0 * F(3) + F(1)) + c10 * (F(6) - 2.0 * F(3) - F(2))).v;
         }
         if (bcn == 0) {
-            if (i == n - 2) return a_np_3 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 3)) + b_np_3 * (F(n) - 2.0 * F(n - 2) + F(n - 4));
-            if (i == n - 1) return a_np_2 * (F(n) - 2.0 * F(n - 1) + F(n - 2));
-            return a_np_1 * F(n) + b_np_1 * F(n - 1) + c_np_1 * F(n - 2) + d_np_1 * F(n - 3) + e_np_1 * F(n - 4);
+            if (i == n - 2) return (a_np_3 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 3)) + b_np_3 * (F(n) - 2.0 * F(n - 2) + F(n - 4))).v;
+            if (i == n - 1) return (a_np_2 * (F(n) - 2.0 * F(n - 1) + F(n - 2))).v;
+            return (a_np_1 * F(n) + b_np_1 * F(n - 1) + c_np_1 * F(n - 2) + d_np_1 * F(n - 3) + e_np_1 * F(n - 4)).v;
         }
         if (bcn == 1) {
-            if (i == n - 2) return a10 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 3)) + b10 * (F(n) - 2.0 * F(n - 2) + F(n - 4)) + c10 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 5));
-            if (i == n - 1) return a10 * (F(n) - 2.0 * F(n - 1) + F(n - 2)) + b10 * (F(n - 1) - 2.0 * F(n - 1) + F(n - 3)) + c10 * (F(n - 2) - 2.0 * F(n - 1) + F(n - 4));
-            return a10 * (F(n - 1) - 2.0 * F(n) + F(n - 1)) + b10 * (F(n - 2) - 2.0 * F(n) + F(n - 2)) + c10 * (F(n - 3) - 2.0 * F(n) + F(n - 3));
+            if (i == n - 2) return (a10 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 3)) + b10 * (F(n) - 2.0 * F(n - 2) + F(n - 4)) + c10 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 5))).v;
+            if (i == n - 1) return (a10 * (F(n) - 2.0 * F(n - 1) + F(n - 2)) + b10 * (F(n - 1) - 2.0 * F(n - 1) + F(n - 3)) + c10 * (F(n - 2) - 2.0 * F(n - 1) + F(n - 4))).v;
+            return (a10 * (F(n - 1) - 2.0 * F(n) + F(n - 1)) + b10 * (F(n - 2) - 2.0 * F(n) + F(n - 2)) + c10 * (F(n - 3) - 2.0 * F(n) + F(n - 3))).v;
         }
-        if (i == n - 2) return a10 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 3)) + b10 * (F(n) - 2.0 * F(n - 2) + F(n - 4)) + c10 * (-F(n - 1) - 2.0 * F(n - 2) + F(n - 5));
-        if (i == n - 1) return a10 * (F(n) - 2.0 * F(n - 1) + F(n - 2)) + b10 * (-F(n - 1) - 2.0 * F(n - 1) + F(n - 3)) + c10 * (-F(n - 2) - 2.0 * F(n - 1) + F(n - 4));
-        return a10 * (-F(n - 1) - 2.0 * F(n) + F(n - 1)) + b10 * (-F(n - 2) - 2.0 * F(n) + F(n - 2)) + c10 * (-F(n - 3) - 2.0 * F(n) + F(n - 3));
+        if (i == n - 2) return (a10 * (F(n - 1) - 2.0 * F(n - 2) + F(n - 3)) + b10 * (F(n) - 2.0 * F(n - 2) + F(n - 4)) + c10 * (-F(n - 1) - 2.0 * F(n - 2) + F(n - 5))).v;
+        if (i == n - 1) return (a10 * (F(n) - 2.0 * F(n - 1) + F(n - 2)) + b10 * (-F(n - 1) - 2.0 * F(n - 1) + F(n - 3)) + c10 * (-F(n - 2) - 2.0 * F(n - 1) + F(n - 4))).v;
+        return (a10 * (-F(n - 1) - 2.0 * F(n) + F(n - 1)) + b10 * (-F(n - 2) - 2.0 * F(n) + F(n - 2)) + c10 * (-F(n - 3) - 2.0 * F(n) + F(n - 3))).v;
     }
     default: {
         // cf90.F90:673-798
-        const double a90 = c[0], b90 = c[1], c90 = c[2], d90 = c[3], e90 = c[4];
-        const double b2_a = c[5], b2_b = c[6], b3_a = c[7], b3_b = c[8], b3_c = c[9], b4_a = c[10], b4_b = c[11],
-                     b4_c = c[12], b4_d = c[13];
+        const NC a90(c[0]), b90(c[1]), c90(c[2]), d90(c[3]), e90(c[4]);
+        const NC b2_a(c[5]), b2_b(c[6]), b3_a(c[7]), b3_b(c[8]), b3_c(c[9]), b4_a(c[10]), b4_b(c[11]), b4_c(c[12]),
+                         b4_d(c[13]);
         if (left) {
             if (bc1 == 0) {
-                if (i == 1) return 1.0 * (F(1));
-                if (i == 2) return b2_a * (F(2)) + b2_b * (F(3) + F(1));
-                if (i == 3) return b3_a * (F(3)) + b3_b * (F(4) + F(2)) + b3_c * (F(5) + F(1));
-                return b4_a * (F(4)) + b4_b * (F(5) + F(3)) + b4_c * (F(6) + F(2)) + b4_d * (F(7) + F(1));
+                if (i == 1) return (1.0 * (F(1))).v;
+                if (i == 2) return (b2_a * (F(2)) + b2_b * (F(3) + F(1))).v;
+                if (i == 3) return (b3_a * (F(3)) + b3_b * (F(4) + F(2)) + b3_c * (F(5) + F(1))).v;
+                return (b4_a * (F(4)) + b4_b * (F(5) + F(3)) + b4_c * (F(6) + F(2)) + b4_d * (F(7) + F(1))).v;
             }
             if (bc1 == 1) {
-                if (i == 1) return a90 * (F(1)) + b90 * (F(2) + F(2)) + c90 * (F(3) + F(3)) + d90 * (F(4) + F(4)) + e90 * (F(5) + F(5));
-                if (i == 2) return a90 * (F(2)) + b90 * (F(3) + F(1)) + c90 * (F(4) + F(2)) + d90 * (F(5) + F(3)) + e90 * (F(6) + F(4));
-                if (i == 3) return a90 * (F(3)) + b90 * (F(4) + F(2)) + c90 * (F(5) + F(1)) + d90 * (F(6) + F(2)) + e90 * (F(7) + F(3));
-                return a90 * (F(4)) + b90 * (F(5) + F(3)) + c90 * (F(6) + F(2)) + d90 * (F(7) + F(1)) + e90 * (F(8) + F(2));
+                if (i == 1) return (a90 * (F(1)) + b90 * (F(2) + F(2)) + c90 * (F(3) + F(3)) + d90 * (F(4) + F(4)) + e90 * (F(5) + F(5))).v;
+                if (i == 2) return (a90 * (F(2)) + b90 * (F(3) + F(1)) + c90 * (F(4) + F(2)) + d90 * (F(5) + F(3)) + e90 * (F(6) + F(4))).v;
+                if (i == 3) return (a90 * (F(3)) + b90 * (F(4) + F(2)) + c90 * (F(5) + F(1)) + d90 * (F(6) + F(2)) + e90 * (F(7) + F(3))).v;
+                return (a90 * (F(4)) + b90 * (F(5) + F(3)) + c90 * (F(6) + F(2)) + d90 * (F(7) + F(1)) + e90 * (F(8) + F(2))).v;
             }
-            if (i == 1) return a90 * (F(1)) + b90 * (F(2) - F(2)) + c90 * (F(3) - F(3)) + d90 * (F(4) - F(4)) + e90 * (F(5) - F(5));
-            if (i == 2) return a90 * (F(2)) + b90 * (F(3) + F(1)) + c90 * (F(4) - F(2)) + d90 * (F(5) - F(3)) + e90 * (F(6) - F(4));
-            if (i == 3) return a90 * (F(3)) + b90 * (F(4) + F(2)) + c90 * (F(5) + F(1)) + d90 * (F(6) - F(2)) + e90 * (F(7) - F(3));
-            return a90 * (F(4)) + b90 * (F(5) + F(3)) + c90 * (F(6) + F(2)) + d90 * (F(7) + F(1)) + e90 * (F(8) - F(2));
+            if (i == 1) return (a90 * (F(1)) + b90 * (F(2) - F(2)) + c90 * (F(3) - F(3)) + d90 * (F(4) - F(4)) + e90 * (F(5) - F(5))).v;
+            if (i == 2) return (a90 * (F(2)) + b90 * (F(3) + F(1)) + c90 * (F(4) - F(2)) + d90 * (F(5) - F(3)) + e90 * (F(6) - F(4))).v;
+            if (i == 3) return (a90 * (F(3)) + b90 * (F(4) + F(2)) + c90 * (F(5) + F(1)) + d90 * (F(6) - F(2)) + e90 * (F(7) - F(3))).v;
+            return (a90 * (F(4)) + b90 * (F(5) + F(3)) + c90 * (F(6) + F(2)) + d90 * (F(7) + F(1)) + e90 * (F(8) - F(2))).v;
         }
         if (bcn == 0) {
-            if (i == n - 3) return b4_a * (F(n - 3)) + b4_b * (F(n - 2) + F(n - 4)) + b4_c * (F(n - 1) + F(n - 5)) + b4_d * (F(n) + F(n - 6));
-            if (i == n - 2) return b3_a * (F(n - 2)) + b3_b * (F(n - 1) + F(n - 3)) + b3_c * (F(n) + F(n - 4));
-            if (i == n - 1) return b2_a * (F(n - 1)) + b2_b * (F(n) + F(n - 2));
-            return 1.0 * (F(n));
+            if (i == n - 3) return (b4_a * (F(n - 3)) + b4_b * (F(n - 2) + F(n - 4)) + b4_c * (F(n - 1) + F(n - 5)) + b4_d * (F(n) + F(n - 6))).v;
+            if (i == n - 2) return (b3_a * (F(n - 2)) + b3_b * (F(n - 1) + F(n - 3)) + b3_c * (F(n) + F(n - 4))).v;
+            if (i == n - 1) return (b2_a * (F(n - 1)) + b2_b * (F(n) + F(n - 2))).v;
+            return (1.0 * (F(n))).v;
         }
         if (bcn == 1) {
-            if (i == n - 3) return a90 * (F(n - 3)) + b90 * (F(n - 2) + F(n - 4)) + c90 * (F(n - 1) + F(n - 5)) + d90 * (F(n) + F(n - 6)) + e90 * (F(n - 1) + F(n - 7));
-            if (i == n - 2) return a90 * (F(n - 2)) + b90 * (F(n - 1) + F(n - 3)) + c90 * (F(n) + F(n - 4)) + d90 * (F(n - 1) + F(n - 5)) + e90 * (F(n - 2) + F(n - 6));
-            if (i == n - 1) return a90 * (F(n - 1)) + b90 * (F(n) + F(n - 2)) + c90 * (F(n - 1) + F(n - 3)) + d90 * (F(n - 2) + F(n - 4)) + e90 * (F(n - 3) + F(n - 5));
-            return a90 * (F(n)) + b90 * (F(n - 1) + F(n - 1)) + c90 * (F(n - 2) + F(n - 2)) + d90 * (F(n - 3) + F(n - 3)) + e90 * (F(n - 4) + F(n - 4));
+            if (i == n - 3) return (a90 * (F(n - 3)) + b90 * (F(n - 2) + F(n - 4)) + c90 * (F(n - 1) + F(n - 5)) + d90 * (F(n) + F(n - 6)) + e90 * (F(n - 1) + F(n - 7))).v;
+            if (i == n - 2) return (a90 * (F(n - 2)) + b90 * (F(n - 1) + F(n - 3)) + c90 * (F(n) + F(n - 4)) + d90 * (F(n - 1) + F(n - 5)) + e90 * (F(n - 2) + F(n - 6))).v;
+            if (i == n - 1) return (a90 * (F(n - 1)) + b90 * (F(n) + F(n - 2)) + c90 * (F(n - 1) + F(n - 3)) + d90 * (F(n - 2) + F(n - 4)) + e90 * (F(n - 3) + F(n - 5))).v;
+            return (a90 * (F(n)) + b90 * (F(n - 1) + F(n - 1)) + c90 * (F(n - 2) + F(n - 2)) + d90 * (F(n - 3) + F(n - 3)) + e90 * (F(n - 4) + F(n - 4))).v;
         }
-        if (i == n - 3) return a90 * (F(n - 3)) + b90 * (F(n - 2) + F(n - 4)) + c90 * (F(n - 1) + F(n - 5)) + d90 * (F(n) + F(n - 6)) + e90 * (-F(n - 1) + F(n - 7));
-        if (i == n - 2) return a90 * (F(n - 2)) + b90 * (F(n - 1) + F(n - 3)) + c90 * (F(n) + F(n - 4)) + d90 * (-F(n - 1) + F(n - 5)) + e90 * (-F(n - 2) + F(n - 6));
-        if (i == n - 1) return a90 * (F(n - 1)) + b90 * (F(n) + F(n - 2)) + c90 * (-F(n - 1) + F(n - 3)) + d90 * (-F(n - 2) + F(n - 4)) + e90 * (-F(n - 3) + F(n - 5));
-        return a90 * (F(n)) + b90 * (-F(n - 1) + F(n - 1)) + c90 * (-F(n - 2) + F(n - 2)) + d90 * (-F(n - 3) + F(n - 3)) + e90 * (-F(n - 4) + F(n - 4));
+        if (i == n - 3) return (a90 * (F(n - 3)) + b90 * (F(n - 2) + F(n - 4)) + c90 * (F(n - 1) + F(n - 5)) + d90 * (F(n) + F(n - 6)) + e90 * (-F(n - 1) + F(n - 7))).v;
+        if (i == n - 2) return (a90 * (F(n - 2)) + b90 * (F(n - 1) + F(n - 3)) + c90 * (F(n) + F(n - 4)) + d90 * (-F(n - 1) + F(n - 5)) + e90 * (-F(n - 2) + F(n - 6))).v;
+        if (i == n - 1) return (a90 * (F(n - 1)) + b90 * (F(n) + F(n - 2)) + c90 * (-F(n - 1) + F(n - 3)) + d90 * (-F(n - 2) + F(n - 4)) + e90 * (-F(n - 3) + F(n - 5))).v;
+        return (a90 * (F(n)) + b90 * (-F(n - 1) + F(n - 1)) + c90 * (-F(n - 2) + F(n - 2)) + d90 * (-F(n - 3) + F(n - 3)) + e90 * (-F(n - 4) + F(n - 4))).v;
     }
     }
 #undef F

@@ -30,7 +30,24 @@ KernelFn pick_m(int m, bool adj, bool contiguous, int variant)
     }
 }
 
+template <bool PER, bool XL>
+StreamFn pick_stream_m(int m)
+{
+    constexpr int RK = 2;
+    switch (m) {
+    case 16: return stream_kernel<RK, PER, 16, XL>;
+    case 32: return stream_kernel<RK, PER, 32, XL>;
+    default: return stream_kernel<RK, PER, 64, XL>;
+    }
+}
+
 }  // namespace
+
+StreamFn pick_stream_rk2(bool per, int m, bool xl)
+{
+    if (per) return xl ? pick_stream_m<true, true>(m) : pick_stream_m<true, false>(m);
+    return xl ? pick_stream_m<false, true>(m) : pick_stream_m<false, false>(m);
+}
 
 KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant)
 {

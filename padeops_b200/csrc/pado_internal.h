@@ -11,23 +11,24 @@
 
 #include "../../include/pado.h"
 #include "pado_kernels.cuh"
+#include "pado_params.h"
+#include "pado_stream.cuh"
 #include "pado_tables.h"
 
 namespace pado {
 
 extern std::atomic<long long> g_launches;
 
-// Device-resident tables of one (kind, bc1, bcn, direction) operator.
+// Device-resident tables of one (kind, bc1, bcn, direction) operator, and
+// the host copy they were uploaded from.
 struct DevTables {
-    double *tab = nullptr;     // [nb][T_NF]
-    double *segsum = nullptr;  // [S][4]
-    double *bt = nullptr;      // transposed stencil blocks (adjoint, bounded)
-    double mb[4] = {0, 0, 0, 0};
-    double taps[9] = {0};
-    int nb = 0, nbord = 0;
-    Layout lay;
-    RhsCoef rc{};
-    Interior interior;  // constant-coefficient segments for tiling m
+    OpTables host;
+    double *tab = nullptr;         // [nb][T_NF]
+    double *ctab = nullptr;        // [S][CT_NF]
+    double *ctab_exact = nullptr;  // [S][CT_NF], every segment on the per-row table
+    double *etab = nullptr;        // packed rows of the segments that read the table
+    int *toff = nullptr;           // [S]
+    double *bt = nullptr;          // transposed stencil blocks (adjoint, bounded)
 };
 
 using TabKey = std::tuple<int, int, int, int>;  // kind, bc1, bcn, adjoint
@@ -42,8 +43,9 @@ struct pado_op_s {
     int scheme = 0, n = 0, periodic = 1, bc1 = 0, bcn = 0;
     double dx = 1.0;
     int m = 32, lines = 16;
-    int variant = 1;  // 1: one CTA per tile, 2: persistent CTAs with cp.async prefetch
+    int variant = 0;  // 0: automatic; 1..3: one-CTA-per-tile / persistent kernels; 4: streaming kernel
     int device = 0;
+    int *d_status = nullptr;  // device-side status word (bounded waits)
     std::map<pado::TabKey, pado::DevTables> tables;
     std::vector<void *> allocations;
     // host-buffer staging
@@ -63,8 +65,15 @@ KernelFn pick_kernel_rk0(bool per, bool adj, bool contiguous, int m, int variant
 KernelFn pick_kernel_rk1(bool per, bool adj, bool contiguous, int m, int variant);
 KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant);
 KernelFn pick_kernel_rk3(bool per, bool adj, bool contiguous, int m, int variant);
+using StreamFn = void (*)(const StreamParams);
+StreamFn pick_stream_rk0(bool per, int m, bool xl);
+StreamFn pick_stream_rk1(bool per, int m, bool xl);
+StreamFn pick_stream_rk2(bool per, int m, bool xl);
+StreamFn pick_stream_rk3(bool per, int m, bool xl);
 
+// no_fast: every segment on the per-row table (for kernels built for a
+// segment length other than the handle's).
 int prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
-                   int bcn, bool adjoint, int lines, KParams *kp, bool *trivial);
+                   int bcn, bool adjoint, int lines, bool no_fast, KParams *kp, bool *trivial);
 
 }  // namespace pado

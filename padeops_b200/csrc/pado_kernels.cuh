@@ -33,6 +33,9 @@
 
 namespace pado {
 
+constexpr int KMAXM = 64;  // longest segment (MAXM of pado_tables.h)
+constexpr int KCT_NF = 12; // chain coefficients per segment (CT_NF of pado_tables.h)
+
 // Parameters of one launch (passed by value).
 struct KParams {
     const double *in;
@@ -46,7 +49,7 @@ struct KParams {
     int L;                 // lines per CTA
     int bc1, bcn;
     const double *tab;     // [nb][T_NF]
-    const double *segsum;  // [S][4]
+    const double *ctab;    // [S][KCT_NF] chain coefficients
     const double *bt;      // adjoint: transposed stencil blocks (bounded)
     double mb[4];
     double taps[9];        // adjoint: interior transposed taps
@@ -54,7 +57,7 @@ struct KParams {
     // constant-coefficient interior (see Interior in pado_tables.h)
     unsigned int_mask;     // bit s: segment s takes the register-only path
     double kc[8];          // alpha, c1, c2, gamma, d1, d2, delta
-    double pat[8];         // U(m-1), V(m-1), U(m-2), V(m-2), S(0), T(0), S(1), T(1)
+    double pu[KMAXM], pv[KMAXM], ps[KMAXM], pt[KMAXM];  // unit responses, rows 0..m-1
 };
 
 PADO_HD PADO_INLINE int seg_start(const KParams &kp, int s) { return s * kp.base + (s < kp.rem ? s : kp.rem); }
@@ -65,18 +68,22 @@ PADO_HD PADO_INLINE long long line_base(const KParams &kp, long long q)
 }
 
 // Shared-memory carve-up (doubles).  The tile is only allocated by kernels
-// that use it (x lines, and every adjoint).
+// that use it.  etab/toff: the per-row table of the segments that read it,
+// staged in shared memory by the persistent kernel (null: read kp.tab).
 struct Smem {
-    double *buf4;  // [S][L][4]  forward summaries, later backward summaries
-    double *buf2;  // [S][L][2]  forward incoming states, later backward ones
-    double *eb;    // [L][4]     border unknowns E (0..1) and border rhs (2..3)
-    double *tile;  // [L][P]
+    double *buf4;        // [S][L][4]  forward summaries, later backward summaries
+    double *buf2;        // [S][L][2]  forward incoming states, later backward ones
+    double *eb;          // [L][4]     border unknowns E (0..1) and border rhs (2..3)
+    double *ctab;        // [S][KCT_NF] chain coefficients
+    double *tile;        // [L][P] or [n][L]
+    const double *etab;  // packed table rows of the segments that read the table
+    const int *toff;     // [S] first packed row of each segment
 };
 
 // tile_doubles: 0 (no tile), L*P ([L][P] tile) or n*L ([n][L] tile)
 PADO_HD PADO_INLINE size_t smem_doubles(int L, int S, size_t tile_doubles)
 {
-    return (size_t)S * L * 6 + (size_t)L * 4 + tile_doubles;
+    return (size_t)S * L * 6 + (size_t)L * 4 + (size_t)S * KCT_NF + tile_doubles;
 }
 
 PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S)
@@ -85,10 +92,24 @@ PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S)
     sm.buf4 = base;
     sm.buf2 = sm.buf4 + (size_t)S * L * 4;
     sm.eb = sm.buf2 + (size_t)S * L * 2;
-    sm.tile = sm.eb + (size_t)L * 4;
+    sm.ctab = sm.eb + (size_t)L * 4;
+    sm.tile = sm.ctab + (size_t)S * KCT_NF;
+    sm.etab = nullptr;
+    sm.toff = nullptr;
     (void)P;
     return sm;
 }
+
+// Where one line's input comes from and its output goes (set per thread by
+// the kernel driver): row r of the input is src[r * ss], of the output
+// dst[r * ds].  live: the line exists (the last tile may be partial).
+struct LineIO {
+    const double *src;
+    long long ss;
+    double *dst;
+    long long ds;
+    bool live;
+};
 
 // Per-thread segment values: M rows plus the 8-row stencil window margin.
 template <int M>
@@ -206,6 +227,26 @@ inline
 
 enum InputSource { IN_GLOBAL = 0, IN_ROWS = 1, IN_LINES = 2 };
 
+// Table rows of segment s (first row a): the staged copy or global memory.
+PADO_HD PADO_INLINE const double *seg_table(const KParams &kp, const Smem &sm, int s, int a)
+{
+    return sm.etab ? sm.etab + (size_t)sm.toff[s] * T_NF : kp.tab + (size_t)a * T_NF;
+}
+
+// Table loads: read-only cache for global memory, plain loads for shared memory.
+template <bool STAGED>
+PADO_HD PADO_INLINE double tld(const double *p)
+{
+    if (STAGED) return *p;
+    return PADO_LDG(p);
+}
+template <bool STAGED>
+PADO_HD PADO_INLINE Dbl2 tld2(const double *p)
+{
+    if (STAGED) return Dbl2{p[0], p[1]};
+    return ldg2(p);
+}
+
 template <int RK, bool PER, bool ADJ, int M, int IN>
 struct LineKernel {
     static constexpr bool CYC = PER;
@@ -214,22 +255,24 @@ struct LineKernel {
     // only its adjoint scales the output (delta != 1)
     static constexpr bool HAS_ALPHA = RK == RHS_CD06_D1 && !PER && !ADJ;
     static constexpr bool HAS_DELTA = RK == RHS_CD06_D1 && !PER && ADJ;
+    static_assert(M <= KMAXM, "segment longer than the response tables");
 
     static PADO_HD PADO_INLINE bool fast(const KParams &kp, int s) { return (kp.int_mask >> s) & 1u; }
 
     // ---- constant-coefficient interior segment: stencil + forward sweep ----
     static PADO_HD PADO_INLINE void fwd_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s,
-                                             const double *gline, long long gs)
+                                             const LineIO &io)
     {
         const int a = seg_start(kp, s);
+        const long long gs = io.ss;
         if (!ADJ) {
-            const double *p = gline + (long long)(a - 4) * gs;
+            const double *p = io.src + (long long)(a - 4) * gs;
 #pragma unroll
             for (int j = 0; j < M + 8; ++j) R.r[j] = p[(long long)j * gs];
 #pragma unroll
             for (int t = 0; t < M; ++t) R.r[t] = rhs_interior(RK, PER, kp.rc.c, &R.r[t]);
         } else {
-            const double *p = gline + (long long)a * gs;
+            const double *p = io.src + (long long)a * gs;
 #pragma unroll
             for (int t = 0; t < M; ++t) R.r[t] = p[(long long)t * gs];
         }
@@ -252,24 +295,18 @@ struct LineKernel {
     }
 
     // ---- constant-coefficient interior segment: backward sweep -------------
+    // forward values = local + P1*U + P2*V (the incoming state's response)
     static PADO_HD PADO_INLINE void bwd_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
     {
         const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-        const double c1 = kp.kc[1], c2 = kp.kc[2], ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
-        // forward values: local solution + homogeneous solution from the incoming state
-        double h1 = st[0], h2 = st[1];
-#pragma unroll
-        for (int t = 0; t < M; ++t) {
-            double h = -c1 * h1;
-            if (ORDER2) h -= c2 * h2;
-            R.r[t] += h;
-            h2 = h1;
-            h1 = h;
-        }
+        const double ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
+        const double P1 = st[0], P2 = st[1];
         double x1 = 0.0, x2 = 0.0;
 #pragma unroll
         for (int t = M - 1; t >= 0; --t) {
-            double x = ga * R.r[t];
+            double z = R.r[t] + P1 * kp.pu[t];
+            if (ORDER2) z += P2 * kp.pv[t];
+            double x = ga * z;
             if (ORDER2) x -= d2 * x2;
             x -= d1 * x1;
             R.r[t] = x;
@@ -283,42 +320,36 @@ struct LineKernel {
 
     // ---- constant-coefficient interior segment: corrections + output ------
     static PADO_HD PADO_INLINE void fin_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s,
-                                             double *line, long long gs)
+                                             const LineIO &io)
     {
         const int a = seg_start(kp, s);
         const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-        const double d1 = kp.kc[4], d2 = kp.kc[5], de = kp.kc[6];
-        double g1 = st[0], g2 = st[1];
-        double *p = line + (long long)a * gs;
+        const double de = kp.kc[6];
+        const double Q1 = st[0], Q2 = st[1];
+        double *p = io.dst + (long long)a * io.ds;
 #pragma unroll
-        for (int t = M - 1; t >= 0; --t) {
-            double g = -d1 * g1;
-            if (ORDER2) g -= d2 * g2;
-            double x = R.r[t] + g;
+        for (int t = 0; t < M; ++t) {
+            double x = R.r[t] + Q1 * kp.ps[t];
+            if (ORDER2) x += Q2 * kp.pt[t];
             if (HAS_DELTA) x *= de;
-            p[(long long)t * gs] = x;
-            g2 = g1;
-            g1 = g;
+            p[(long long)t * io.ds] = x;
         }
     }
 
     static PADO_HD PADO_INLINE int wrap(int row, int n) { return row < 0 ? row + n : (row >= n ? row - n : row); }
 
     // ---- phase fwd: right-hand side (primal) + local forward sweep ---------
-    static PADO_HD PADO_INLINE void fwd(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, long long q0)
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE void fwd(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, const LineIO &io)
     {
         const int n = kp.n, nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;  // banded rows of this segment
-        const long long q = q0 + l;
-        const bool live = q < kp.nlines;
-        // source line: global (strided), a tile column [n][L] or a tile row [L][P]
-        const double *gline = IN == IN_GLOBAL ? kp.in + line_base(kp, live ? q : 0)
-                            : IN == IN_ROWS   ? sm.tile + l
-                                              : sm.tile + (size_t)l * kp.P;
-        const long long gs = IN == IN_GLOBAL ? kp.stride : IN == IN_ROWS ? kp.L : 1;
+        const bool live = io.live;
+        const double *gline = io.src;
+        const long long gs = io.ss;
         if (fast(kp, s)) {
-            fwd_fast(kp, sm, R, l, s, gline, gs);
+            fwd_fast(kp, sm, R, l, s, io);
             return;
         }
         if (!ADJ) {
@@ -368,20 +399,20 @@ struct LineKernel {
         }
         // local forward sweep with zero incoming state
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
-        const double *tb = kp.tab + (size_t)a * T_NF;
+        const double *tb = seg_table(kp, sm, s, a);
 #pragma unroll
         for (int t = 0; t < M; ++t) {
             if (t < lenb) {
                 const double *tr = tb + (size_t)t * T_NF;
-                const Dbl2 cc = ldg2(tr + T_C1);
-                const Dbl2 ak = (HAS_ALPHA || CYC) ? ldg2(tr + T_ALPHA) : Dbl2{1.0, 0.0};
+                const Dbl2 cc = tld2<STAGED>(tr + T_C1);
+                const Dbl2 ak = (HAS_ALPHA || CYC) ? tld2<STAGED>(tr + T_ALPHA) : Dbl2{1.0, 0.0};
                 double z = HAS_ALPHA ? ak.x * R.r[t] : R.r[t];
                 if (ORDER2) z -= cc.y * z2;
                 z -= cc.x * z1;
                 R.r[t] = z;
                 if (CYC) {
                     s1 += ak.y * z;
-                    if (ORDER2) s2 += PADO_LDG(tr + T_K2) * z;
+                    if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
                 }
                 z2 = z1;
                 z1 = z;
@@ -406,31 +437,43 @@ struct LineKernel {
     }
 
     // ---- phase chainF: forward incoming states + border ------------------
+    // One thread per line walks the segments; the summaries and coefficients
+    // of four segments are read before any state is written, so the shared
+    // memory latency is paid once per four segments.
     static PADO_HD PADO_INLINE void chain_fwd(const KParams &kp, const Smem &sm, int l)
     {
         double P1 = 0.0, P2 = 0.0, sg1 = 0.0, sg2 = 0.0;
-        const int S = kp.S;
-#pragma unroll 4
-        for (int s = 0; s < S; ++s) {
-            const double *in4 = sm.buf4 + ((size_t)s * kp.L + l) * 4;
-            const double zl = in4[0], zl2 = in4[1];
-            double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-            st[0] = P1;
-            st[1] = P2;
-            if (CYC) {
-                const Dbl2 s01 = ldg2(kp.segsum + (size_t)s * 4), s23 = ldg2(kp.segsum + (size_t)s * 4 + 2);
-                sg1 += in4[2] + P1 * s01.x + P2 * s01.y;
-                sg2 += in4[3] + P1 * s23.x + P2 * s23.y;
+        const int S = kp.S, L = kp.L;
+        for (int s0 = 0; s0 < S; s0 += 4) {
+            double zl[4], zl2[4], sa[4], sb[4], c[4][8];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int s = s0 + j < S ? s0 + j : S - 1;
+                const double *in4 = sm.buf4 + ((size_t)s * L + l) * 4;
+                const double *ct = sm.ctab + (size_t)s * KCT_NF;
+                zl[j] = in4[0];
+                zl2[j] = in4[1];
+                sa[j] = CYC ? in4[2] : 0.0;
+                sb[j] = CYC ? in4[3] : 0.0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) c[j][k] = (CYC || k < 4) ? ct[k] : 0.0;
             }
-            if (s + 1 < S) {
-                const int b = seg_start(kp, s + 1);  // segments before the last are fully banded
-                const bool f = fast(kp, s);
-                const Dbl2 uv1 = f ? Dbl2{kp.pat[0], kp.pat[1]} : ldg2(kp.tab + (size_t)(b - 1) * T_NF + T_U);
-                const Dbl2 uv2 = f ? Dbl2{kp.pat[2], kp.pat[3]} : ldg2(kp.tab + (size_t)(b - 2) * T_NF + T_U);
-                const double n1 = zl + P1 * uv1.x + P2 * uv1.y;
-                const double n2 = zl2 + P1 * uv2.x + P2 * uv2.y;
-                P1 = n1;
-                P2 = n2;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int s = s0 + j;
+                if (s < S) {
+                    double *st = sm.buf2 + ((size_t)s * L + l) * 2;
+                    st[0] = P1;
+                    st[1] = P2;
+                    if (CYC) {
+                        sg1 += sa[j] + P1 * c[j][4] + P2 * c[j][5];
+                        sg2 += sb[j] + P1 * c[j][6] + P2 * c[j][7];
+                    }
+                    const double n1 = zl[j] + P1 * c[j][0] + P2 * c[j][1];
+                    const double n2 = zl2[j] + P1 * c[j][2] + P2 * c[j][3];
+                    P1 = n1;
+                    P2 = n2;
+                }
             }
         }
         if (CYC) {
@@ -447,6 +490,7 @@ struct LineKernel {
     }
 
     // ---- phase bwd: local backward sweep ---------------------------------
+    template <bool STAGED>
     static PADO_HD PADO_INLINE void bwd(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
     {
         if (fast(kp, s)) {
@@ -463,21 +507,21 @@ struct LineKernel {
             E1 = sm.eb[(size_t)l * 4 + 0];
             E2 = sm.eb[(size_t)l * 4 + 1];
         }
-        const double *tb = kp.tab + (size_t)a * T_NF;
+        const double *tb = seg_table(kp, sm, s, a);
         double x1 = 0.0, x2 = 0.0;
 #pragma unroll
         for (int t = M - 1; t >= 0; --t) {
             if (t < lenb) {
                 const double *tr = tb + (size_t)t * T_NF;
-                const Dbl2 uv = ldg2(tr + T_U);
-                const Dbl2 gd = ldg2(tr + T_GAMMA);
-                const Dbl2 de = ldg2(tr + T_D2);
+                const Dbl2 uv = tld2<STAGED>(tr + T_U);
+                const Dbl2 gd = tld2<STAGED>(tr + T_GAMMA);
+                const Dbl2 de = tld2<STAGED>(tr + T_D2);
                 double z = R.r[t] + P1 * uv.x;
                 if (ORDER2) z += P2 * uv.y;
                 double x = gd.x * z;
                 if (CYC) {
                     x -= de.y * E1;
-                    if (ORDER2) x -= PADO_LDG(tr + T_E2) * E2;
+                    if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
                 }
                 if (ORDER2) x -= de.x * x2;
                 x -= gd.y * x1;
@@ -495,54 +539,60 @@ struct LineKernel {
     static PADO_HD PADO_INLINE void chain_bwd(const KParams &kp, const Smem &sm, int l)
     {
         double Q1 = 0.0, Q2 = 0.0;
-#pragma unroll 4
-        for (int s = kp.S - 1; s >= 0; --s) {
-            const double *in4 = sm.buf4 + ((size_t)s * kp.L + l) * 4;
-            double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-            st[0] = Q1;
-            st[1] = Q2;
-            if (s > 0) {
-                const int a = seg_start(kp, s);
-                const bool f = fast(kp, s);
-                const Dbl2 st0 = f ? Dbl2{kp.pat[4], kp.pat[5]} : ldg2(kp.tab + (size_t)a * T_NF + T_S);
-                const Dbl2 st1 = f ? Dbl2{kp.pat[6], kp.pat[7]} : ldg2(kp.tab + (size_t)(a + 1) * T_NF + T_S);
-                const double n1 = in4[0] + Q1 * st0.x + Q2 * st0.y;
-                const double n2 = in4[1] + Q1 * st1.x + Q2 * st1.y;
-                Q1 = n1;
-                Q2 = n2;
+        const int S = kp.S, L = kp.L;
+        for (int s0 = S - 1; s0 >= 0; s0 -= 4) {
+            double x0[4], x1[4], c[4][4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int s = s0 - j >= 0 ? s0 - j : 0;
+                const double *in4 = sm.buf4 + ((size_t)s * L + l) * 4;
+                const double *ct = sm.ctab + (size_t)s * KCT_NF + 8;
+                x0[j] = in4[0];
+                x1[j] = in4[1];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) c[j][k] = ct[k];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int s = s0 - j;
+                if (s >= 0) {
+                    double *st = sm.buf2 + ((size_t)s * L + l) * 2;
+                    st[0] = Q1;
+                    st[1] = Q2;
+                    const double n1 = x0[j] + Q1 * c[j][0] + Q2 * c[j][1];
+                    const double n2 = x1[j] + Q1 * c[j][2] + Q2 * c[j][3];
+                    Q1 = n1;
+                    Q2 = n2;
+                }
             }
         }
     }
 
-    // ---- phase fin: corrected values -> df (primal) or the tile (adjoint) --
-    // OUT_TILE: write the result into the [L][P] tile (adjoint, and x lines
-    // whose tile is then stored with coalesced accesses) instead of global memory
-    template <bool OUT_TILE = ADJ>
-    static PADO_HD PADO_INLINE void fin(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, long long q0)
+    // ---- phase fin: corrected values -> the line's output -----------------
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE void fin(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, const LineIO &io)
     {
         const int nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;
         const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
         const double Q1 = st[0], Q2 = st[1];
-        const double *tb = kp.tab + (size_t)a * T_NF;
-        const long long q = q0 + l;
-        const bool to_global = !OUT_TILE;
-        if (to_global && q >= kp.nlines) return;
-        double *line = to_global ? kp.out + line_base(kp, q) : sm.tile + (size_t)l * kp.P;
-        const long long gs = to_global ? kp.stride : 1;
+        if (!io.live) return;
+        double *line = io.dst;
+        const long long gs = io.ds;
         if (fast(kp, s)) {
-            fin_fast(kp, sm, R, l, s, line, gs);
+            fin_fast(kp, sm, R, l, s, io);
             return;
         }
+        const double *tb = seg_table(kp, sm, s, a);
 #pragma unroll
         for (int t = 0; t < M; ++t) {
             if (t < lenb) {
                 const double *tr = tb + (size_t)t * T_NF;
-                const Dbl2 stt = ldg2(tr + T_S);
+                const Dbl2 stt = tld2<STAGED>(tr + T_S);
                 double x = R.r[t] + Q1 * stt.x;
                 if (ORDER2) x += Q2 * stt.y;
-                if (HAS_DELTA) x = PADO_LDG(tr + T_DELTA) * x;
+                if (HAS_DELTA) x = tld<STAGED>(tr + T_DELTA) * x;
                 line[(long long)(a + t) * gs] = x;
             }
         }
@@ -585,16 +635,13 @@ struct LineKernel {
     }
 
     // ---- phase adjoint output ----------------------------------------------
-    static PADO_HD PADO_INLINE void adj_out(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s, long long q0)
+    static PADO_HD PADO_INLINE void adj_out(const KParams &kp, Regs<M> &R, int s, const LineIO &io)
     {
         const int a = seg_start(kp, s), len = seg_len(kp, s);
-        const long long q = q0 + l;
-        if (q >= kp.nlines) return;
-        double *line = kp.out + line_base(kp, q);
-        const long long gs = kp.stride;
+        if (!io.live) return;
 #pragma unroll
         for (int t = 0; t < M; ++t)
-            if (t < len) line[(long long)(a + t) * gs] = R.r[t];
+            if (t < len) io.dst[(long long)(a + t) * io.ds] = R.r[t];
     }
 };
 
@@ -613,6 +660,29 @@ PADO_HD PADO_INLINE constexpr bool phase_used(int ph)
          : true;
 }
 
+// Line l of the tile starting at line q0, for the one-CTA-per-tile kernels:
+// input from global memory (IN_GLOBAL) or the tile; the sweep's output goes
+// to the [L][P] tile (adjoint, x lines) or to global memory.
+template <bool ADJ, int IN>
+PADO_HD PADO_INLINE LineIO tile_line_io(const KParams &kp, const Smem &sm, int l, long long q0)
+{
+    const long long q = q0 + l;
+    LineIO io;
+    io.live = q < kp.nlines;
+    const long long base = line_base(kp, io.live ? q : 0);
+    io.src = IN == IN_GLOBAL ? kp.in + base : IN == IN_ROWS ? sm.tile + l : sm.tile + (size_t)l * kp.P;
+    io.ss = IN == IN_GLOBAL ? kp.stride : IN == IN_ROWS ? kp.L : 1;
+    const bool out_tile = ADJ || IN == IN_LINES;
+    io.dst = out_tile ? sm.tile + (size_t)l * kp.P : kp.out + base;
+    io.ds = out_tile ? 1 : kp.stride;
+    return io;
+}
+
+PADO_HD PADO_INLINE void stage_chain_table(const KParams &kp, const Smem &sm, int tid, int nthreads)
+{
+    for (int i = tid; i < kp.S * KCT_NF; i += nthreads) sm.ctab[i] = kp.ctab[i];
+}
+
 // One tile of kp.L lines on a CTA of nthreads threads (nthreads >= L*S;
 // extra threads only help with the tile load).
 template <int RK, bool PER, bool ADJ, int M, int IN>
@@ -624,13 +694,22 @@ PADO_HD PADO_INLINE void tile_phase(int phase, const KParams &kp, const Smem &sm
     const bool active = s < kp.S;
     switch (phase) {
     case PH_LOAD: tile_load(kp, sm, q0, tid, nthreads); break;
-    case PH_FWD: if (active) K::fwd(kp, sm, R, l, s, q0); break;
+    case PH_FWD:
+        stage_chain_table(kp, sm, tid, nthreads);
+        if (active) K::template fwd<false>(kp, sm, R, l, s, tile_line_io<ADJ, IN>(kp, sm, l, q0));
+        break;
     case PH_CHAINF: if (s == 0) K::chain_fwd(kp, sm, l); break;
-    case PH_BWD: if (active) K::bwd(kp, sm, R, l, s); break;
+    case PH_BWD: if (active) K::template bwd<false>(kp, sm, R, l, s); break;
     case PH_CHAINB: if (s == 0) K::chain_bwd(kp, sm, l); break;
-    case PH_FIN: if (active) K::template fin<ADJ || IN == IN_LINES>(kp, sm, R, l, s, q0); break;
+    case PH_FIN: if (active) K::template fin<false>(kp, sm, R, l, s, tile_line_io<ADJ, IN>(kp, sm, l, q0)); break;
     case PH_ADJ_STENCIL: if (active) K::adj_stencil(kp, sm, R, l, s); break;
-    case PH_ADJ_OUT: if (active) K::adj_out(kp, sm, R, l, s, q0); break;
+    case PH_ADJ_OUT:
+        if (active) {
+            const long long q = q0 + l;
+            const LineIO io{nullptr, 0, kp.out + line_base(kp, q < kp.nlines ? q : 0), kp.stride, q < kp.nlines};
+            K::adj_out(kp, R, s, io);
+        }
+        break;
     default: tile_store(kp, sm, q0, tid, nthreads); break;
     }
 }
@@ -762,23 +841,29 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
     const long long ntiles = (kp.nlines + kp.L - 1) / kp.L;
     Regs<M> R;
     long long t = blockIdx.x;
+    stage_chain_table(kp, sm, tid, nthreads);
     if (IN != IN_GLOBAL && t < ntiles) tile_prefetch<IN>(kp, sm, t * kp.L, tid, nthreads);
     copy_async_commit();
     for (; t < ntiles; t += gridDim.x) {
         const long long q0 = t * kp.L;
         if (IN != IN_GLOBAL) copy_async_wait_all();
         __syncthreads();
-        if (active) K::fwd(kp, sm, R, l, s, q0);
+        const LineIO io = tile_line_io<false, IN>(kp, sm, l, q0);
+        if (active) K::template fwd<false>(kp, sm, R, l, s, io);
         __syncthreads();
         if (t + gridDim.x < ntiles) tile_prefetch<IN>(kp, sm, (t + gridDim.x) * kp.L, tid, nthreads);
         copy_async_commit();
         if (s == 0) K::chain_fwd(kp, sm, l);
         __syncthreads();
-        if (active) K::bwd(kp, sm, R, l, s);
+        if (active) K::template bwd<false>(kp, sm, R, l, s);
         __syncthreads();
         if (s == 0) K::chain_bwd(kp, sm, l);
         __syncthreads();
-        if (active) K::template fin<false>(kp, sm, R, l, s, q0);
+        // results go straight to global memory (the tile already holds the next input)
+        LineIO out = io;
+        out.dst = kp.out + line_base(kp, io.live ? q0 + l : 0);
+        out.ds = kp.stride;
+        if (active) K::template fin<false>(kp, sm, R, l, s, out);
     }
 }
 #endif

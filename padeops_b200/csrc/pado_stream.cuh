@@ -1,0 +1,353 @@
+// pado_stream.cuh -- the streaming line kernel: persistent CTAs that stage
+// whole tiles of lines in shared memory with the tensor memory accelerator
+// (TMA), two tiles ahead, so HBM streams continuously while the CTA runs the
+// sweep of the current tile.
+//
+// One CTA per SM walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// through `stages` shared-memory buffers, each guarded by an mbarrier:
+//
+//   wait(full[b])  fwd (stencil + local forward sweep, reads the buffer)
+//   barrier        strided lines: buffer b is free -> issue the load of the
+//                  tile `stages` ahead into it
+//   chainF, bwd, chainB, fin (results to global memory from registers)
+//   x lines:       fin writes the buffer; bulk store of each line; then the
+//                  load `stages` ahead is issued into the buffer
+//
+// Strided lines (y, z): one 3-D tensor copy per box of {L lines, box_rows
+// rows} lands as the [row][L] tile.  Contiguous lines (x): one bulk copy per
+// line into a [L][P] tile (P = n + 2, rows 16-byte aligned), written back
+// by bulk stores.  The per-row table of the segments that read it and the
+// chain coefficients are staged in shared memory once per CTA.  Every wait
+// is bounded (2 s); on expiry the CTA records PADO_E_TIMEOUT in *status,
+// waits (bounded) for its copies in flight and returns.
+#pragma once
+
+#include <cuda.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "pado_kernels.cuh"
+
+namespace pado {
+
+constexpr int PADO_STATUS_TIMEOUT = -7;  // PADO_E_TIMEOUT of pado.h
+
+struct alignas(64) StreamParams {
+    CUtensorMap tmap;   // strided lines: 3-D view of the input field
+    KParams kp;
+    long long ntiles;
+    long long pstride;  // strided lines: elements between consecutive planes
+    int na;             // strided lines: extent of the contiguous axis
+    int xblocks;        // strided lines: tiles per plane, ceil(na / L)
+    int axis;           // 1, 2, 3
+    int stages;
+    int box_rows, nbox; // strided lines: rows per tensor copy, copies per tile
+    int tile_doubles;   // per stage (a multiple of 16)
+    int etab_rows;      // packed table rows staged in shared memory
+    const double *etab; // [etab_rows][T_NF]
+    const int *toff;    // [S]
+    int *status;        // PADO_E_TIMEOUT on a wait that expired
+};
+
+// Shared-memory layout, offsets in doubles from a 1024-byte aligned base.
+struct StreamLayout {
+    size_t tiles, work, etab, toff, bars, total_doubles;
+};
+
+PADO_HD PADO_INLINE StreamLayout stream_layout(int L, int S, int stages, int tile_doubles, int etab_rows)
+{
+    StreamLayout o;
+    o.tiles = 0;
+    o.work = (size_t)stages * tile_doubles;
+    o.etab = o.work + smem_doubles(L, S, 0);
+    o.toff = o.etab + (size_t)etab_rows * T_NF;
+    o.bars = o.toff + (size_t)(S + 1) / 2;
+    o.total_doubles = o.bars + (size_t)stages;
+    return o;
+}
+
+PADO_HD PADO_INLINE size_t stream_smem_bytes(int L, int S, int stages, int tile_doubles, int etab_rows)
+{
+    return stream_layout(L, S, stages, tile_doubles, etab_rows).total_doubles * sizeof(double) + 1024;
+}
+
+// Line l of strided tile t: plane p, lines x0 .. x0+L-1 of that plane.
+PADO_HD PADO_INLINE void stream_tile_origin(const StreamParams &sp, long long t, long long *x0, long long *p)
+{
+    if (sp.axis == 1) {
+        *x0 = t * sp.kp.L;
+        *p = 0;
+    } else {
+        *x0 = (t % sp.xblocks) * sp.kp.L;
+        *p = t / sp.xblocks;
+    }
+}
+
+PADO_HD PADO_INLINE LineIO stream_line_io(const StreamParams &sp, const Smem &sm, int l, long long t)
+{
+    const KParams &kp = sp.kp;
+    long long x0, p;
+    stream_tile_origin(sp, t, &x0, &p);
+    LineIO io;
+    if (sp.axis == 1) {
+        io.live = x0 + l < kp.nlines;
+        io.src = sm.tile + (size_t)l * kp.P;
+        io.ss = 1;
+        io.dst = sm.tile + (size_t)l * kp.P;
+        io.ds = 1;
+    } else {
+        const long long x = x0 + l;
+        io.live = x < sp.na;
+        io.src = sm.tile + l;
+        io.ss = kp.L;
+        io.dst = kp.out + (io.live ? x + p * sp.pstride : 0);
+        io.ds = kp.stride;
+    }
+    return io;
+}
+
+PADO_HD PADO_INLINE int stream_tile_lines(const StreamParams &sp, long long t)
+{
+    long long x0, p;
+    stream_tile_origin(sp, t, &x0, &p);
+    const long long lim = sp.axis == 1 ? sp.kp.nlines : sp.na;
+    const long long nl = lim - x0;
+    return (int)(nl < sp.kp.L ? nl : sp.kp.L);
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Bounded wait for the phase `parity` of an mbarrier.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned long long limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int c0, int c1,
+                                            int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+constexpr unsigned long long STREAM_WAIT_NS = 2000000000ull;  // 2 s
+constexpr unsigned long long STREAM_DRAIN_NS = 200000000ull;  // 0.2 s
+
+// Issue the copies of tile t into stage buffer `tile` (one thread).
+__device__ __forceinline__ void stream_issue_load(const StreamParams &sp, double *tile, unsigned long long *bar,
+                                                  long long t)
+{
+    const KParams &kp = sp.kp;
+    long long x0, p;
+    stream_tile_origin(sp, t, &x0, &p);
+    if (sp.axis == 1) {
+        const int nl = stream_tile_lines(sp, t);
+        const unsigned bytes = (unsigned)kp.n * 8u;
+        mbar_expect_tx(bar, bytes * (unsigned)nl);
+        for (int l = 0; l < nl; ++l)
+            bulk_load(tile + (size_t)l * kp.P, kp.in + (x0 + l) * (long long)kp.n, bytes, bar);
+    } else {
+        mbar_expect_tx(bar, (unsigned)sp.nbox * sp.box_rows * kp.L * 8u);
+        for (int b = 0; b < sp.nbox; ++b) {
+            const int r0 = b * sp.box_rows;
+            double *dst = tile + (size_t)r0 * kp.L;
+            if (sp.axis == 2) tma_load_3d(dst, &sp.tmap, bar, (int)x0, r0, (int)p);
+            else tma_load_3d(dst, &sp.tmap, bar, (int)x0, (int)p, r0);
+        }
+    }
+}
+
+template <int RK, bool PER, int M, bool XL>
+__global__ void __launch_bounds__(256, 1) stream_kernel(const __grid_constant__ StreamParams sp)
+{
+    using K = LineKernel<RK, PER, false, M, XL ? IN_LINES : IN_ROWS>;
+    extern __shared__ double smem_raw[];
+    double *base = reinterpret_cast<double *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~(size_t)1023);
+    const KParams &kp = sp.kp;
+    const int L = kp.L, S = kp.S;
+    const StreamLayout lay = stream_layout(L, S, sp.stages, sp.tile_doubles, sp.etab_rows);
+    Smem sm = carve(base + lay.work, L, kp.P, S);
+    double *etab = base + lay.etab;
+    int *toff = reinterpret_cast<int *>(base + lay.toff);
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + lay.bars);
+    sm.etab = etab;
+    sm.toff = toff;
+
+    const int tid = threadIdx.x, nthreads = blockDim.x;
+    const int l = tid % L, s = tid / L;
+    const bool active = s < S;
+    const long long G = gridDim.x;
+    const long long t_first = blockIdx.x;
+    const int stages = sp.stages;
+
+    if (tid == 0) {
+        for (int b = 0; b < stages; ++b) mbar_init(&bars[b], 1);
+        mbar_fence_init();
+    }
+    for (int i = tid; i < S * KCT_NF; i += nthreads) sm.ctab[i] = kp.ctab[i];
+    for (int i = tid; i < sp.etab_rows * T_NF; i += nthreads) etab[i] = __ldg(sp.etab + i);
+    for (int i = tid; i < S; i += nthreads) toff[i] = __ldg(sp.toff + i);
+    __syncthreads();
+    if (tid == 0) {
+        for (int b = 0; b < stages; ++b) {
+            const long long t = t_first + b * G;
+            if (t < sp.ntiles) stream_issue_load(sp, base + (size_t)b * sp.tile_doubles, &bars[b], t);
+        }
+    }
+
+    Regs<M> R;
+    long long k = 0;
+    for (long long t = t_first; t < sp.ntiles; t += G, ++k) {
+        const int b = (int)(k % stages);
+        const unsigned parity = (unsigned)((k / stages) & 1);
+        const bool ok = __syncthreads_and(mbar_wait(&bars[b], parity, STREAM_WAIT_NS));
+        if (!ok) {
+            // record, let the copies in flight land, and leave
+            if (tid == 0) {
+                atomicExch(sp.status, PADO_STATUS_TIMEOUT);
+                for (int j = 0; j < stages; ++j) {
+                    const long long kk = k + j;
+                    if (t + j * G < sp.ntiles)
+                        (void)mbar_wait(&bars[kk % stages], (unsigned)((kk / stages) & 1), STREAM_DRAIN_NS);
+                }
+            }
+            if (XL) bulk_wait_all();
+            return;
+        }
+        sm.tile = base + (size_t)b * sp.tile_doubles;
+        const LineIO io = stream_line_io(sp, sm, l, t);
+        if (active) K::template fwd<true>(kp, sm, R, l, s, io);
+        __syncthreads();
+        const long long tn = t + (long long)stages * G;  // tile for this buffer next
+        if (!XL && tid == 0 && tn < sp.ntiles) stream_issue_load(sp, sm.tile, &bars[b], tn);
+        if (s == 0) K::chain_fwd(kp, sm, l);
+        __syncthreads();
+        if (active) K::template bwd<true>(kp, sm, R, l, s);
+        __syncthreads();
+        if (s == 0) K::chain_bwd(kp, sm, l);
+        __syncthreads();
+        if (active) K::template fin<true>(kp, sm, R, l, s, io);
+        if (XL) {
+            // each line's results -> global memory, then the buffer takes the next load
+            fence_proxy_async();
+            __syncthreads();
+            const int nl = stream_tile_lines(sp, t);
+            if (tid < nl) {
+                bulk_store(kp.out + (t * L + tid) * (long long)kp.n, sm.tile + (size_t)tid * kp.P, (unsigned)kp.n * 8u);
+                bulk_commit();
+                bulk_wait_read();
+            }
+            __syncthreads();
+            if (tid == 0 && tn < sp.ntiles) stream_issue_load(sp, sm.tile, &bars[b], tn);
+        }
+    }
+    if (XL) bulk_wait_all();
+}
+#endif  // __CUDACC__
+
+// Host emulation (tests): the kernel's tile loop with plain copies standing
+// in for the tensor / bulk copies; phases in kernel order over all threads.
+template <int RK, bool PER, int M, bool XL>
+inline void emulate_stream(const StreamParams &sp, int nthreads)
+{
+    using K = LineKernel<RK, PER, false, M, XL ? IN_LINES : IN_ROWS>;
+    const KParams &kp = sp.kp;
+    const int L = kp.L, S = kp.S;
+    const StreamLayout lay = stream_layout(L, S, 1, sp.tile_doubles, sp.etab_rows);
+    std::vector<double> mem(lay.total_doubles, 0.0);
+    double *base = mem.data();
+    Smem sm = carve(base + lay.work, L, kp.P, S);
+    double *etab = base + lay.etab;
+    int *toff = reinterpret_cast<int *>(base + lay.toff);
+    for (int i = 0; i < S * KCT_NF; ++i) sm.ctab[i] = kp.ctab[i];
+    for (int i = 0; i < sp.etab_rows * T_NF; ++i) etab[i] = sp.etab[i];
+    for (int i = 0; i < S; ++i) toff[i] = sp.toff[i];
+    sm.etab = etab;
+    sm.toff = toff;
+    sm.tile = base;
+    std::vector<Regs<M>> R(nthreads);
+    for (long long t = 0; t < sp.ntiles; ++t) {
+        long long x0, p;
+        stream_tile_origin(sp, t, &x0, &p);
+        const int nl = stream_tile_lines(sp, t);
+        // the copy engine's view: full boxes, zero outside the field
+        std::fill(sm.tile, sm.tile + sp.tile_doubles, 0.0);
+        for (int ll = 0; ll < L; ++ll) {
+            if (ll >= nl) continue;
+            for (int r = 0; r < kp.n; ++r) {
+                if (XL) sm.tile[(size_t)ll * kp.P + r] = kp.in[(x0 + ll) * kp.n + r];
+                else sm.tile[(size_t)r * L + ll] = kp.in[x0 + ll + p * sp.pstride + (long long)r * kp.stride];
+            }
+        }
+        for (int ph = 0; ph < 5; ++ph) {
+            for (int tid = 0; tid < nthreads; ++tid) {
+                const int l = tid % L, s = tid / L;
+                const bool active = s < S;
+                const LineIO io = stream_line_io(sp, sm, l, t);
+                switch (ph) {
+                case 0: if (active) K::template fwd<true>(kp, sm, R[tid], l, s, io); break;
+                case 1: if (s == 0) K::chain_fwd(kp, sm, l); break;
+                case 2: if (active) K::template bwd<true>(kp, sm, R[tid], l, s); break;
+                case 3: if (s == 0) K::chain_bwd(kp, sm, l); break;
+                default: if (active) K::template fin<true>(kp, sm, R[tid], l, s, io); break;
+                }
+            }
+        }
+        if (XL)
+            for (int ll = 0; ll < nl; ++ll)
+                for (int r = 0; r < kp.n; ++r) kp.out[(x0 + ll) * kp.n + r] = sm.tile[(size_t)ll * kp.P + r];
+    }
+}
+
+}  // namespace pado

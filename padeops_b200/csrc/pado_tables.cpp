@@ -481,28 +481,95 @@ Interior interior_info(const Sweep &sw, const Layout &lay, int m)
     in.i1 = i1;
     for (int k = 0; k < 7; ++k) in.kc[k] = ref[k];
     const double c1 = ref[1], c2 = ref[2], d1 = ref[4], d2 = ref[5];
+    if (m > MAXM) return in;
     // unit responses of a length-m segment under the constant recurrences
-    double z1 = 1.0, z2 = 0.0, y1 = 0.0, y2 = 1.0, zl = 0, zl2 = 0, yl = 0, yl2 = 0;
+    double z1 = 1.0, z2 = 0.0, y1 = 0.0, y2 = 1.0;
     for (int t = 0; t < m; ++t) {
         const double z = -c1 * z1 - c2 * z2, y = -c1 * y1 - c2 * y2;
-        if (t == m - 2) { zl2 = z; yl2 = y; }
-        if (t == m - 1) { zl = z; yl = y; }
+        in.pu[t] = z;
+        in.pv[t] = y;
         z2 = z1; z1 = z; y2 = y1; y1 = y;
     }
-    double x1 = 1.0, x2 = 0.0, w1 = 0.0, w2 = 1.0, x0 = 0, xs1 = 0, w0 = 0, ws1 = 0;
+    double x1 = 1.0, x2 = 0.0, w1 = 0.0, w2 = 1.0;
     for (int t = m - 1; t >= 0; --t) {
         const double x = -d1 * x1 - d2 * x2, w = -d1 * w1 - d2 * w2;
-        if (t == 1) { xs1 = x; ws1 = w; }
-        if (t == 0) { x0 = x; w0 = w; }
+        in.ps[t] = x;
+        in.pt[t] = w;
         x2 = x1; x1 = x; w2 = w1; w1 = w;
     }
-    const double pat[8] = {zl, yl, zl2, yl2, x0, w0, xs1, ws1};
-    for (int k = 0; k < 8; ++k) in.pat[k] = pat[k];
     for (int s = 1; s + 1 < lay.S && s < 32; ++s) {
         const int a = lay.start(s), len = lay.len(s);
         if (len == m && a >= i0 && a + len <= i1 && a >= HALO && a + len + HALO <= sw.n) in.mask |= 1u << s;
     }
     return in;
+}
+
+std::vector<double> chain_table(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay,
+                                int nb, const Interior &in, int m)
+{
+    std::vector<double> ct((size_t)lay.S * CT_NF, 0.0);
+    auto T = [&](int i, int f) { return tab[(size_t)i * T_NF + f]; };
+    for (int s = 0; s < lay.S; ++s) {
+        double *c = &ct[(size_t)s * CT_NF];
+        const bool fast = (in.mask >> s) & 1u;
+        const int a = lay.start(s);
+        for (int k = 0; k < 4; ++k) c[4 + k] = segsum[(size_t)s * 4 + k];
+        if (s + 1 < lay.S) {
+            const int b = lay.start(s + 1);  // segments before the last are fully banded
+            c[0] = fast ? in.pu[m - 1] : T(b - 1, T_U);
+            c[1] = fast ? in.pv[m - 1] : T(b - 1, T_V);
+            c[2] = fast ? in.pu[m - 2] : T(b - 2, T_U);
+            c[3] = fast ? in.pv[m - 2] : T(b - 2, T_V);
+        }
+        if (s > 0) {
+            c[8] = fast ? in.ps[0] : T(a, T_S);
+            c[9] = fast ? in.pt[0] : T(a, T_T);
+            c[10] = fast ? in.ps[1] : (a + 1 < nb ? T(a + 1, T_S) : 0.0);
+            c[11] = fast ? in.pt[1] : (a + 1 < nb ? T(a + 1, T_T) : 0.0);
+        }
+    }
+    return ct;
+}
+
+void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, std::vector<double> &etab,
+                std::vector<int> &toff)
+{
+    etab.clear();
+    toff.assign(lay.S, 0);
+    int rows = 0;
+    for (int s = 0; s < lay.S; ++s) {
+        if ((mask >> s) & 1u) continue;
+        const int a = lay.start(s), b = std::min(a + lay.len(s), nb);
+        toff[s] = rows;
+        for (int i = a; i < b; ++i, ++rows)
+            etab.insert(etab.end(), tab.begin() + (size_t)i * T_NF, tab.begin() + (size_t)(i + 1) * T_NF);
+    }
+}
+
+OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, bool adjoint)
+{
+    OpTables ot;
+    const Sweep prim = primal_sweep(scheme, kind, n, periodic, bc1, bcn);
+    const Sweep sw = adjoint ? adjoint_sweep(prim) : prim;
+    ot.nb = sw.nb;
+    ot.nbord = sw.nbord;
+    ot.m = m;
+    std::memcpy(ot.mb, sw.mb, sizeof(ot.mb));
+    ot.rc = make_rhs_coef(scheme, kind, dx, periodic);
+    ot.lay = make_layout(n, m);
+    std::vector<double> segsum;
+    build_device_table(sw, ot.lay, ot.tab, segsum);
+    ot.interior = interior_info(sw, ot.lay, m);
+    ot.ctab = chain_table(ot.tab, segsum, ot.lay, sw.nb, ot.interior, m);
+    ot.ctab_exact = chain_table(ot.tab, segsum, ot.lay, sw.nb, Interior{}, m);
+    edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask, ot.etab, ot.toff);
+    if (adjoint) {
+        double taps[9];
+        interior_taps(ot.rc, taps);
+        for (int k = 0; k < 9; ++k) ot.taps[k] = taps[8 - k];
+        if (!periodic) ot.bt = transposed_stencil_blocks(ot.rc, n, bc1, bcn);
+    }
+    return ot;
 }
 
 std::vector<double> stencil_matrix(const RhsCoef &rc, int n, int bc1, int bcn)

@@ -52,16 +52,48 @@ void build_device_table(const Sweep &sw, const Layout &lay, std::vector<double> 
 // the cyclic spike terms decay to nothing.  Segments that lie wholly in that
 // region, have length m and a full stencil window inside the line run a
 // register-only path: constant coefficients, and the inter-segment
-// corrections computed by the homogeneous recurrence itself.
+// corrections read from the unit responses below.
+constexpr int MAXM = 64;  // longest segment a kernel is built for
 struct Interior {
     unsigned mask = 0;       // bit s: segment s takes the constant-coefficient path
     double kc[8] = {0};      // alpha, c1, c2, gamma, d1, d2, delta, (unused)
-    // responses of a length-m segment to unit incoming states:
-    // U(m-1), V(m-1), U(m-2), V(m-2), S(0), T(0), S(1), T(1)
-    double pat[8] = {0};
+    // responses of a length-m segment, rows t = 0..m-1: forward sweep to the
+    // unit incoming states z_{-1} (pu) and z_{-2} (pv); backward sweep to
+    // x_m (ps) and x_{m+1} (pt)
+    double pu[MAXM] = {0}, pv[MAXM] = {0}, ps[MAXM] = {0}, pt[MAXM] = {0};
     int i0 = 0, i1 = 0;      // banded rows treated as interior
 };
 Interior interior_info(const Sweep &sw, const Layout &lay, int m);
+
+// Chain coefficients, CT_NF per segment s:
+//   0..3   U(b-1), V(b-1), U(b-2), V(b-2): forward transfer to segment s+1
+//   4..7   k1.U, k1.V, k2.U, k2.V summed over the segment (cyclic sums)
+//   8..11  S(a), T(a), S(a+1), T(a+1): backward transfer to segment s-1
+// (a, b: first row of segment s and of segment s+1).  Constant-coefficient
+// segments take the responses of Interior.
+constexpr int CT_NF = 12;
+std::vector<double> chain_table(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay,
+                                int nb, const Interior &in, int m);
+
+// Rows of the segments that read the per-row table, packed in segment order;
+// toff[s] = first packed row of segment s (0 for constant-coefficient ones).
+void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, std::vector<double> &etab,
+                std::vector<int> &toff);
+
+// Everything a kernel launch reads for one (scheme, kind, closures,
+// direction) operator, on the host.
+struct OpTables {
+    int nb = 0, nbord = 0, m = 0;
+    double mb[4] = {0, 0, 0, 0};
+    double taps[9] = {0};  // adjoint: transposed interior taps (tap at offset o is c_{-o})
+    Layout lay;
+    RhsCoef rc{};
+    Interior interior;
+    std::vector<double> tab, ctab, etab, bt;
+    std::vector<double> ctab_exact;  // chain coefficients with every segment on the per-row table
+    std::vector<int> toff;
+};
+OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, bool adjoint);
 
 // Transposed stencil of a bounded line: B^T rows for the first and last
 // ZB columns.  Dense (n x n) when n <= DENSE_BT_MAX.

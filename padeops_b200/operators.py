@@ -99,8 +99,16 @@ class _Scheme:
         check(L.lib().pado_set_tiling(self.handle, m, lines), "set_tiling")
 
     def set_variant(self, variant: int) -> None:
-        """1 = one CTA per tile of lines, 2 = persistent CTAs with prefetch."""
+        """0 = automatic, 1 = one CTA per tile of lines, 2/3 = persistent CTAs
+        with prefetch, 4 = the streaming (TMA-fed) kernel."""
         check(L.lib().pado_set_kernel_variant(self.handle, variant), "set_variant")
+
+    def device_status(self, clear: bool = True) -> int:
+        """Status recorded by this handle's kernels (0, or PADO_E_TIMEOUT)."""
+        rc = int(L.lib().pado_device_status(self.handle, 1 if clear else 0))
+        if rc not in (L.OK, L.E_TIMEOUT):
+            check(rc, "device_status")
+        return rc
 
     def get_tiling(self) -> tuple[int, int]:
         m, lines = ctypes.c_int(), ctypes.c_int()

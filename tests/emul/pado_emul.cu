@@ -6,6 +6,8 @@
 #include <vector>
 
 #include "../../padeops_b200/csrc/pado_kernels.cuh"
+#include "../../padeops_b200/csrc/pado_params.h"
+#include "../../padeops_b200/csrc/pado_stream.cuh"
 #include "../../padeops_b200/csrc/pado_tables.h"
 
 using namespace pado;
@@ -48,51 +50,90 @@ extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, 
                           int extra_threads, int adjoint, int axis, const double *f, double *df, long na, long nb,
                           int fast)
 {
-    const Sweep prim = primal_sweep(scheme, kind, n, periodic, bc1, bcn);
-    const Sweep sw = adjoint ? adjoint_sweep(prim) : prim;
-    const RhsCoef rc = make_rhs_coef(scheme, kind, dx, periodic);
-    const Layout lay = make_layout(n, m);
+    const OpTables ot = make_op_tables(scheme, kind, n, dx, periodic, bc1, bcn, m, adjoint != 0);
+    const Layout &lay = ot.lay;
     if ((lay.S > 1 && lay.base + (lay.rem ? 1 : 0) > m) || lay.base + 1 > m + 1) return -6;
-    std::vector<double> tab, segsum, bt;
-    build_device_table(sw, lay, tab, segsum);
     KParams kp{};
+    fill_params(kp, ot, n, bc1, bcn);
     kp.in = f;
     kp.out = df;
-    kp.nlines = (long long)na * nb;
-    if (axis == 1) { kp.line_ia = 1; kp.line_oc = n; kp.stride = 1; }
-    else if (axis == 2) { kp.line_ia = na; kp.line_oc = (long long)na * n; kp.stride = na; }
-    else { kp.line_ia = kp.nlines; kp.line_oc = 0; kp.stride = (long long)na * nb; }
-    kp.n = n;
-    kp.nb = sw.nb;
-    kp.nbord = sw.nbord;
-    kp.P = (n % 2 == 0) ? n + 1 : n;
-    kp.S = lay.S;
-    kp.base = lay.base;
-    kp.rem = lay.rem;
+    set_geometry(kp, axis, n, na, nb);
     kp.L = lines;
-    kp.bc1 = bc1;
-    kp.bcn = bcn;
-    kp.tab = tab.data();
-    kp.segsum = segsum.data();
-    std::memcpy(kp.mb, sw.mb, sizeof(kp.mb));
-    double taps[9];
-    interior_taps(rc, taps);
-    for (int k = 0; k < 9; ++k) kp.taps[k] = taps[8 - k];
-    if (adjoint && !periodic) {
-        bt = transposed_stencil_blocks(rc, n, bc1, bcn);
-        kp.bt = bt.data();
-    }
-    kp.rc = rc;
-    const Interior in = interior_info(sw, lay, m);
-    kp.int_mask = fast ? in.mask : 0u;
-    std::memcpy(kp.kc, in.kc, sizeof(kp.kc));
-    std::memcpy(kp.pat, in.pat, sizeof(kp.pat));
+    kp.tab = ot.tab.data();
+    kp.ctab = fast ? ot.ctab.data() : ot.ctab_exact.data();
+    kp.bt = ot.bt.empty() ? nullptr : ot.bt.data();
+    if (!fast) kp.int_mask = 0u;
     const int nthreads = lines * lay.S + extra_threads;
-    switch (rc.rk) {
+    switch (ot.rc.rk) {
     case RHS_CD06_D1: return pick<RHS_CD06_D1>(kp, periodic, adjoint, m, nthreads);
     case RHS_CD10_D1: return pick<RHS_CD10_D1>(kp, periodic, adjoint, m, nthreads);
     case RHS_CD10_D2: return pick<RHS_CD10_D2>(kp, periodic, adjoint, m, nthreads);
     default: return pick<RHS_CF90>(kp, periodic, adjoint, m, nthreads);
+    }
+}
+
+// The streaming kernel's tile loop (primal): tiles of `lines` lines, x
+// lines through the [L][n+2] tile, y/z lines through the [row][L] tile.
+template <int RK, bool PER>
+static int stream_pick(const StreamParams &sp, int m, bool xl, int nthreads)
+{
+    switch (m * 2 + (xl ? 1 : 0)) {
+    case 32: emulate_stream<RK, PER, 16, false>(sp, nthreads); return 0;
+    case 33: emulate_stream<RK, PER, 16, true>(sp, nthreads); return 0;
+    case 64: emulate_stream<RK, PER, 32, false>(sp, nthreads); return 0;
+    case 65: emulate_stream<RK, PER, 32, true>(sp, nthreads); return 0;
+    case 128: emulate_stream<RK, PER, 64, false>(sp, nthreads); return 0;
+    case 129: emulate_stream<RK, PER, 64, true>(sp, nthreads); return 0;
+    }
+    return -1;
+}
+
+extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, int lines,
+                           int axis, const double *f, double *df, long na, long nb)
+{
+    const OpTables ot = make_op_tables(scheme, kind, n, dx, periodic, bc1, bcn, m, false);
+    const Layout &lay = ot.lay;
+    if ((lay.S > 1 && lay.base + (lay.rem ? 1 : 0) > m) || lay.base + 1 > m + 1) return -6;
+    StreamParams sp;
+    std::memset(&sp, 0, sizeof(sp));
+    KParams &kp = sp.kp;
+    fill_params(kp, ot, n, bc1, bcn);
+    kp.in = f;
+    kp.out = df;
+    set_geometry(kp, axis, n, na, nb);
+    kp.L = lines;
+    kp.tab = ot.tab.data();
+    kp.ctab = ot.ctab.data();
+    const bool xl = axis == 1;
+    sp.axis = axis;
+    sp.stages = 1;
+    sp.etab_rows = (int)(ot.etab.size() / T_NF);
+    sp.etab = ot.etab.data();
+    sp.toff = ot.toff.data();
+    if (xl) {
+        kp.P = n + 2;
+        sp.tile_doubles = (lines * kp.P + 15) / 16 * 16;
+        sp.ntiles = (kp.nlines + lines - 1) / lines;
+    } else {
+        sp.nbox = (n + 255) / 256;
+        sp.box_rows = ((n + sp.nbox - 1) / sp.nbox + 15) / 16 * 16;
+        sp.tile_doubles = (sp.nbox * sp.box_rows * lines + 15) / 16 * 16;
+        sp.na = (int)na;
+        sp.xblocks = (int)((na + lines - 1) / lines);
+        sp.ntiles = (long long)sp.xblocks * nb;
+        sp.pstride = axis == 2 ? na * (long long)n : na;
+    }
+    const int nthreads = lines * lay.S;
+    const bool per = periodic != 0;
+    switch (ot.rc.rk) {
+    case RHS_CD06_D1:
+        return per ? stream_pick<RHS_CD06_D1, true>(sp, m, xl, nthreads) : stream_pick<RHS_CD06_D1, false>(sp, m, xl, nthreads);
+    case RHS_CD10_D1:
+        return per ? stream_pick<RHS_CD10_D1, true>(sp, m, xl, nthreads) : stream_pick<RHS_CD10_D1, false>(sp, m, xl, nthreads);
+    case RHS_CD10_D2:
+        return per ? stream_pick<RHS_CD10_D2, true>(sp, m, xl, nthreads) : stream_pick<RHS_CD10_D2, false>(sp, m, xl, nthreads);
+    default:
+        return per ? stream_pick<RHS_CF90, true>(sp, m, xl, nthreads) : stream_pick<RHS_CF90, false>(sp, m, xl, nthreads);
     }
 }
 

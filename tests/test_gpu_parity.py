@@ -117,6 +117,48 @@ def test_parity_tilings(torch_cuda, m, lines, variant):
                 assert rel_err(got, ref) <= TOL, (axis, scheme, kind, periodic, rel_err(got, ref))
 
 
+@pytest.mark.parametrize("scheme,kind", OPS)
+@pytest.mark.parametrize("periodic", [True, False])
+def test_parity_stream(torch_cuda, scheme, kind, periodic):
+    """The streaming kernel (TMA-fed persistent CTAs) along every axis: line
+    lengths from the minimum to 512, x extents that leave partial tiles."""
+    torch = torch_cuda
+    rng = np.random.default_rng(77)
+    for n in (10, 34, 100, 256, 512):
+        for axis, shape in ((1, (3, 7, n)), (2, (5, n, 22)), (3, (n, 4, 18))):
+            f = rng.standard_normal(shape)
+            op = _make(scheme, n, 0.3, periodic)
+            op.set_variant(4)
+            for bc1, bcn in ([(0, 0)] if periodic or scheme == oracle.CD06 else [(0, 0), (1, -1), (-1, 1)]):
+                got = _gpu_apply(torch, op, kind, axis, f, bc1, bcn)
+                ref = _oracle_apply(scheme, kind, axis, f, 0.3, periodic, bc1, bcn)
+                assert rel_err(got, ref) <= TOL, (n, axis, bc1, bcn, rel_err(got, ref))
+            assert op.device_status() == 0
+
+
+@pytest.mark.parametrize("m", [16, 32, 64])
+def test_parity_stream_tilings(torch_cuda, m):
+    """Streaming kernel with each segment length, and n = 1024 (smooth field:
+    the one-sided closures cancel heavily, the stencils must round like the
+    reference's expressions)."""
+    torch = torch_cuda
+    for n in (256, 1024):
+        for axis, shape in ((1, (2, 3, n)), (3, (n, 3, 40))):
+            f = spectrum53(shape, seed=3 + axis)
+            for scheme, kind in OPS:
+                for periodic in (True, False):
+                    op = _make(scheme, n, 0.05, periodic)
+                    op.set_variant(4)
+                    try:
+                        op.set_tiling(m, 0)
+                    except Exception:
+                        continue  # not a legal shape for this n
+                    bc = (0, 0) if periodic else (-1, 1)
+                    got = _gpu_apply(torch, op, kind, axis, f, *bc)
+                    ref = _oracle_apply(scheme, kind, axis, f, 0.05, periodic, *bc)
+                    assert rel_err(got, ref) <= TOL, (n, axis, scheme, kind, periodic, rel_err(got, ref))
+
+
 def test_config1_cd06_64cube(torch_cuda):
     """cd06 periodic dd1/dd2/dd3 on the 64^3 sum of 8 sinusoids (dx = 2pi/64)."""
     torch = torch_cuda
