@@ -143,6 +143,12 @@ int pado_set_kernel_variant(pado_op_t op, int variant);
  * then stop early and the output is incomplete).  Synchronous (reads device
  * memory); clear != 0 resets the word.  No counterpart in the reference. */
 int pado_device_status(pado_op_t op, int clear);
+/* The kernel a forward apply with these arguments would launch (nothing is
+ * launched): info[0] kernel variant (1..4), [1] lines per tile, [2] stages,
+ * [3] CTAs per SM, [4] segments per line, [5] coupling window, [6] threads
+ * per CTA, [7] dynamic shared memory bytes.  No counterpart in the reference. */
+int pado_launch_plan(pado_op_t op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
+                     int bcn, int *info);
 
 /* ---- batched execution (many fields, one persistent launch) ------------ */
 

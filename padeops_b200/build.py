@@ -20,7 +20,7 @@ LIB = os.path.join(LIBDIR, "libpado.so")
 SOURCES = ["pado_api.cu", "pado_batch.cu", "pado_tables.cpp", "pado_inst_rk0.cu", "pado_inst_rk1.cu",
            "pado_inst_rk2.cu", "pado_inst_rk3.cu"]
 HEADERS = ["pado_common.h", "pado_tables.h", "pado_kernels.cuh", "pado_batch.cuh", "pado_internal.h", "pado_params.h",
-           "pado_stream.cuh"]
+           "pado_stream.cuh", "pado_resident.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr"]

@@ -95,8 +95,10 @@ int build_tables(pado_op_s *op)
                 dt.host = make_op_tables(op->scheme, kind, n, op->dx, op->periodic, cb1, cbn, op->m, dir == 1);
                 const OpTables &h = dt.host;
                 int rc = upload_vec(op, h.tab, &dt.tab);
-                if (rc == PADO_OK) rc = upload_vec(op, h.ctab, &dt.ctab);
-                if (rc == PADO_OK) rc = upload_vec(op, h.ctab_exact, &dt.ctab_exact);
+                if (rc == PADO_OK) rc = upload_vec(op, h.chain.ctab, &dt.ctab);
+                if (rc == PADO_OK) rc = upload_vec(op, h.chain.xtab, &dt.xtab);
+                if (rc == PADO_OK) rc = upload_vec(op, h.chain_exact.ctab, &dt.ctab_exact);
+                if (rc == PADO_OK) rc = upload_vec(op, h.chain_exact.xtab, &dt.xtab_exact);
                 if (rc == PADO_OK) rc = upload_vec(op, h.etab, &dt.etab);
                 if (rc == PADO_OK) rc = upload_vec(op, h.toff, &dt.toff);
                 if (rc == PADO_OK) rc = upload_vec(op, h.bt, &dt.bt);
@@ -150,12 +152,40 @@ StreamFn pick_stream(int rk, bool per, int m, bool xl)
 
 int round16(long long v) { return (int)((v + 15) / 16 * 16); }
 
+// Doubles of one stage buffer: [L][n+2] (x lines) or nbox boxes of
+// box_rows x L (strided lines), rounded to 128 bytes.
+int stream_tile_doubles(bool xl, int n, int L)
+{
+    if (xl) return round16((long long)L * (n + 2));
+    const int nbox = (n + 255) / 256, box_rows = ((n + nbox - 1) / nbox + 15) / 16 * 16;
+    return round16((long long)nbox * box_rows * L);
+}
+
+// Lets a streaming kernel use up to 227 KB of shared memory (once per kernel).
+bool grant_smem(StreamFn fn)
+{
+    static std::mutex mu;
+    static std::map<const void *, bool> granted;
+    std::lock_guard<std::mutex> g(mu);
+    bool &ok = granted[(const void *)fn];
+    if (!ok) {
+        if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) !=
+            cudaSuccess) {
+            (void)cudaGetLastError();
+            return false;
+        }
+        ok = true;
+    }
+    return true;
+}
+
 // Plan of a streaming launch (primal): lines per tile, stages, shared memory
-// and the copy descriptors.  False when the field or tiling does not fit it
-// (odd strides, unaligned pointers, a table too large to stage); the caller
-// then runs the one-CTA-per-tile kernel.
+// and the copy descriptors, chosen for the most resident warps per SM.  False
+// when the field or tiling does not fit it (odd strides, unaligned pointers,
+// a table too large to stage); the caller then runs the one-CTA-per-tile
+// kernel.
 bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, int axis, long long na, long long nb,
-                 StreamParams *sp, int *threads, size_t *smem)
+                 StreamParams *sp, int *threads, size_t *smem, int *ctas_per_sm)
 {
     const int n = op->n, S = kp0.S;
     if (op->m != 16 && op->m != 32 && op->m != 64) return false;
@@ -164,61 +194,70 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     if (align_bits & 15) return false;
     if (xl ? (n % 2 != 0) : (na % 2 != 0 || na > 0x7fffffffLL || nb > 0x7fffffffLL)) return false;
     const int etab_rows = (int)(dt.host.etab.size() / T_NF);
-    for (int L : {32, 16, 8}) {
-        if (L * S > 256) continue;
+    StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl);
+    if (!grant_smem(fn)) return false;
+    int best_warps = 0, bestL = 0, best_stages = 0, best_ctas = 0;
+    for (int L : {16, 32, 8}) {
+        if (L * S > 384) continue;  // the kernel is built for 384 threads, two CTAs per SM
         for (int stages : {2, 1}) {
-            int P = kp0.P, box_rows = 0, nbox = 0, tile_doubles;
-            if (xl) {
-                P = n + 2;  // rows 16-byte aligned for the bulk copies
-                tile_doubles = round16((long long)L * P);
-            } else {
-                // boxes of at most 256 rows; a multiple of 16 rows keeps every
-                // box's shared-memory destination 128-byte aligned for any L
-                nbox = (n + 255) / 256;
-                box_rows = ((n + nbox - 1) / nbox + 15) / 16 * 16;
-                tile_doubles = round16((long long)nbox * box_rows * L);
-            }
-            const size_t bytes = stream_smem_bytes(L, S, stages, tile_doubles, etab_rows);
+            const int tile_doubles = stream_tile_doubles(xl, n, L);
+            const size_t bytes = stream_smem_bytes(L, S, kp0.W, stages, tile_doubles, etab_rows);
             if (bytes > 227 * 1024) continue;
-            std::memset(sp, 0, sizeof(*sp));
-            sp->kp = kp0;
-            sp->kp.L = L;
-            sp->kp.P = P;
-            sp->axis = axis;
-            sp->stages = stages;
-            sp->box_rows = box_rows;
-            sp->nbox = nbox;
-            sp->tile_doubles = tile_doubles;
-            sp->etab_rows = etab_rows;
-            sp->etab = dt.etab;
-            sp->toff = dt.toff;
-            sp->status = op->d_status;
-            if (xl) {
-                sp->ntiles = (kp0.nlines + L - 1) / L;
-            } else {
-                sp->na = (int)na;
-                sp->xblocks = (int)((na + L - 1) / L);
-                sp->ntiles = (long long)sp->xblocks * nb;
-                sp->pstride = axis == 2 ? na * (long long)n : na;
-                EncodeTiledFn enc = encode_tiled();
-                if (!enc) return false;
-                const cuuint64_t dims[3] = {(cuuint64_t)na, (cuuint64_t)(axis == 2 ? n : nb),
-                                            (cuuint64_t)(axis == 2 ? nb : n)};
-                const cuuint64_t strides[2] = {(cuuint64_t)na * 8, (cuuint64_t)na * (axis == 2 ? n : nb) * 8};
-                const cuuint32_t box[3] = {(cuuint32_t)L, (cuuint32_t)(axis == 2 ? box_rows : 1),
-                                           (cuuint32_t)(axis == 2 ? 1 : box_rows)};
-                const cuuint32_t estr[3] = {1, 1, 1};
-                if (enc(&sp->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(kp0.in), dims, strides, box,
-                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-                    return false;
+            int ctas = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, fn, L * S, bytes) != cudaSuccess) {
+                (void)cudaGetLastError();
+                continue;
             }
-            *threads = L * S;
-            *smem = bytes;
-            return true;
+            const int warps = ctas * ((L * S + 31) / 32);
+            if (ctas > 0 && warps > best_warps) {
+                best_warps = warps;
+                bestL = L;
+                best_stages = stages;
+                best_ctas = ctas;
+            }
         }
     }
-    return false;
+    if (!best_warps) return false;
+    const int L = bestL, stages = best_stages;
+    const int tile_doubles = stream_tile_doubles(xl, n, L);
+    std::memset(sp, 0, sizeof(*sp));
+    sp->kp = kp0;
+    sp->kp.L = L;
+    sp->kp.P = xl ? n + 2 : kp0.P;  // x: rows 16-byte aligned for the bulk copies
+    sp->axis = axis;
+    sp->stages = stages;
+    sp->tile_doubles = tile_doubles;
+    sp->etab_rows = etab_rows;
+    sp->etab = dt.etab;
+    sp->toff = dt.toff;
+    sp->status = op->d_status;
+    if (xl) {
+        sp->ntiles = (kp0.nlines + L - 1) / L;
+    } else {
+        // boxes of at most 256 rows; a multiple of 16 rows keeps every box's
+        // shared-memory destination 128-byte aligned for any L
+        sp->nbox = (n + 255) / 256;
+        sp->box_rows = ((n + sp->nbox - 1) / sp->nbox + 15) / 16 * 16;
+        sp->na = (int)na;
+        sp->xblocks = (int)((na + L - 1) / L);
+        sp->ntiles = (long long)sp->xblocks * nb;
+        sp->pstride = axis == 2 ? na * (long long)n : na;
+        EncodeTiledFn enc = encode_tiled();
+        if (!enc) return false;
+        const cuuint64_t dims[3] = {(cuuint64_t)na, (cuuint64_t)(axis == 2 ? n : nb), (cuuint64_t)(axis == 2 ? nb : n)};
+        const cuuint64_t strides[2] = {(cuuint64_t)na * 8, (cuuint64_t)na * (axis == 2 ? n : nb) * 8};
+        const cuuint32_t box[3] = {(cuuint32_t)L, (cuuint32_t)(axis == 2 ? sp->box_rows : 1),
+                                   (cuuint32_t)(axis == 2 ? 1 : sp->box_rows)};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        if (enc(&sp->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(kp0.in), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    *threads = L * S;
+    *smem = stream_smem_bytes(L, S, kp0.W, stages, tile_doubles, etab_rows);
+    *ctas_per_sm = best_ctas;
+    return true;
 }
 
 int sm_count()
@@ -229,22 +268,10 @@ int sm_count()
     return sms > 0 ? sms : 1;
 }
 
-int launch_stream(pado_op_s *op, const StreamParams &sp, int threads, size_t smem, cudaStream_t st)
+int launch_stream(pado_op_s *op, const StreamParams &sp, int threads, size_t smem, int ctas_per_sm, cudaStream_t st)
 {
     StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1);
-    {
-        static std::mutex attr_mu;
-        static std::map<const void *, size_t> granted;
-        std::lock_guard<std::mutex> g(attr_mu);
-        size_t &have = granted[(const void *)fn];
-        if (have < smem) {
-            cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return cuda_fail(e);
-            have = smem;
-        }
-    }
-    const long long grid = std::min<long long>(sp.ntiles, sm_count());
+    const long long grid = std::min<long long>(sp.ntiles, (long long)ctas_per_sm * sm_count());
     if (grid < 1) return PADO_OK;
     fn<<<(unsigned)grid, threads, smem, st>>>(sp);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -283,11 +310,15 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
     kp.L = lines;
     kp.tab = dt.tab;
     kp.ctab = dt.ctab;
+    kp.xtab = dt.xtab;
     kp.bt = dt.bt;
     if (no_fast) {
         // every segment on the per-row table (kernels built for another segment length)
         kp.int_mask = 0;
         kp.ctab = dt.ctab_exact;
+        kp.xtab = dt.xtab_exact;
+        set_chain(kp, dt.host.chain_exact);
+        for (int i = 0; i < 32; ++i) kp.sperm[i] = (unsigned char)i;
     }
     *kpo = kp;
     *trivial = false;
@@ -315,18 +346,19 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
         const bool bounded_bc = !op->periodic && op->scheme != CD06;
         const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, 0));
         StreamParams sp;
-        int sthreads = 0;
+        int sthreads = 0, sctas = 0;
         size_t ssmem = 0;
-        if (plan_stream(op, dt, kp, axis, na, nb, &sp, &sthreads, &ssmem))
-            return launch_stream(op, sp, sthreads, ssmem, st);
+        if (plan_stream(op, dt, kp, axis, na, nb, &sp, &sthreads, &ssmem, &sctas))
+            return launch_stream(op, sp, sthreads, ssmem, sctas, st);
         if (op->variant == 4) return PADO_E_UNSUPPORTED;
     }
+    // lines per CTA: the handle's choice, halved until the segments fit
+    while (kp.L > 1 && kp.L * kp.S > max_threads_for_m(op->m)) kp.L /= 2;
     const int threads = kp.L * kp.S;
-    if (threads > max_threads_for_m(op->m)) return PADO_E_SIZE;
     const bool contiguous = kp.stride == 1;
     const bool persist = !adjoint && (op->variant == 2 || (op->variant == 3 && !contiguous));
     const size_t tile = (adjoint || contiguous) ? (size_t)kp.L * kp.P : (op->variant == 2 ? (size_t)kp.n * kp.L : 0);
-    const size_t smem = smem_doubles(kp.L, kp.S, tile) * sizeof(double);
+    const size_t smem = smem_doubles(kp.L, kp.S, kp.W, tile) * sizeof(double);
     if (smem > 227 * 1024) return PADO_E_SIZE;
     KernelFn fn = pick_kernel(kp.rc.rk, op->periodic != 0, adjoint, contiguous, op->m, op->variant);
     int per_sm = 1;
@@ -489,7 +521,7 @@ int pado_set_tiling(pado_op_t op, int m, int lines)
     if (m) op->m = m;
     if (lines) op->lines = lines;
     const int S = (op->n + op->m - 1) / op->m;
-    if (S > 32 || op->lines * S > max_threads_for_m(op->m)) {
+    if (S > 32) {
         op->m = om;
         op->lines = ol;
         return PADO_E_SIZE;
@@ -503,6 +535,39 @@ int pado_set_kernel_variant(pado_op_t op, int variant)
     if (!op) return PADO_E_NULL;
     if (variant < 0 || variant > 4) return PADO_E_ARG;
     op->variant = variant;
+    return PADO_OK;
+}
+
+int pado_launch_plan(pado_op_t op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
+                     int bcn, int *info)
+{
+    if (!info) return PADO_E_NULL;
+    for (int i = 0; i < 8; ++i) info[i] = 0;
+    KParams kp;
+    bool trivial = true;
+    int rc = prepare_launch(op, kind, axis, f, df, na, nb, bc1, bcn, false, op ? op->lines : 0, false, &kp, &trivial);
+    if (rc != PADO_OK || trivial) return rc;
+    info[4] = kp.S;
+    info[5] = kp.W;
+    if (op->variant == 0 || op->variant == 4) {
+        const bool bounded_bc = !op->periodic && op->scheme != CD06;
+        const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, 0));
+        StreamParams sp;
+        int threads = 0, ctas = 0;
+        size_t smem = 0;
+        if (plan_stream(op, dt, kp, axis, na, nb, &sp, &threads, &smem, &ctas)) {
+            info[0] = 4;
+            info[1] = sp.kp.L;
+            info[2] = sp.stages;
+            info[3] = ctas;
+            info[6] = threads;
+            info[7] = (int)smem;
+            return PADO_OK;
+        }
+    }
+    info[0] = op->variant == 0 ? 1 : op->variant;
+    info[1] = kp.L;
+    info[6] = kp.L * kp.S;
     return PADO_OK;
 }
 

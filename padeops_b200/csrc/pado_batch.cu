@@ -45,28 +45,29 @@ int layout_items(pado_batch_s *b)
         if (ext[it.axis - 1] != it.op->n) return PADO_E_ARG;
         const long long na = it.axis == 1 ? it.n2 : it.n1;
         const long long nb = it.axis == 3 ? it.n2 : it.n3;
-        const int S = (it.op->n + it.op->m - 1) / it.op->m;
-        int L = b->threads / std::max(S, 1);
         const int P = (it.op->n % 2 == 0) ? it.op->n + 1 : it.op->n;
-        while (L > 1 && smem_doubles(L, S, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) --L;
-        if (L < 1) return PADO_E_SIZE;
         KParams kp;
         bool trivial = true;
         // the register-only path assumes segments of BATCH_M rows
-        int rc = prepare_launch(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, false, L,
+        int rc = prepare_launch(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, false, 1,
                                 it.op->m != BATCH_M, &kp, &trivial);
         if (rc != PADO_OK) return rc;
         if (trivial) {
             if (it.op->n == 1 && (long long)na * nb > 0) return PADO_E_UNSUPPORTED;  // n == 1 items: use pado_apply
             continue;
         }
+        const int S = kp.S;
+        int L = b->threads / std::max(S, 1);
+        while (L > 1 && smem_doubles(L, S, kp.W, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) --L;
+        if (L < 1) return PADO_E_SIZE;
+        kp.L = L;
         Pre p{};
         p.d.kp = kp;
         p.d.code = kp.rc.rk * 4 + (it.op->periodic ? 2 : 0) + (kp.stride != 1 ? 1 : 0);
         const long long tiles = (kp.nlines + L - 1) / L;
         p.d.tile0 = tiles;  // temporarily the tile count
         p.cost = (double)L * kp.n;
-        smem = std::max(smem, smem_doubles(L, kp.S, kp.stride == 1 ? (size_t)L * P : 0) * sizeof(double));
+        smem = std::max(smem, smem_doubles(L, kp.S, kp.W, kp.stride == 1 ? (size_t)L * P : 0) * sizeof(double));
         pre.push_back(p);
     }
     std::stable_sort(pre.begin(), pre.end(), [](const Pre &x, const Pre &y) { return x.cost > y.cost; });

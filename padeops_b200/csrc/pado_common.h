@@ -182,7 +182,7 @@ PADO_HD PADO_INLINE double rhs_interior(int rk, int periodic, const double *cc, 
 // `row` is 0-based and lies in the first or last closure_rows(rk) rows.
 // F(j) below is the reference's 1-based f(j).
 // ---------------------------------------------------------------------------
-PADO_HD inline double rhs_closure_row(int rk, const double *c, const double *line, long long stride, int n, int row,
+PADO_HD PADO_INLINE double rhs_closure_row(int rk, const double *c, const double *line, long long stride, int n, int row,
                                       int bc1, int bcn)
 {
 #define F(j) NC(line[(long long)((j)-1) * stride])

@@ -24,8 +24,10 @@ extern std::atomic<long long> g_launches;
 struct DevTables {
     OpTables host;
     double *tab = nullptr;         // [nb][T_NF]
-    double *ctab = nullptr;        // [S][CT_NF]
-    double *ctab_exact = nullptr;  // [S][CT_NF], every segment on the per-row table
+    double *ctab = nullptr;        // [S][CT_NF] border-sum weights
+    double *xtab = nullptr;        // [S][W][8] transfer products
+    double *ctab_exact = nullptr;  // the same with every segment on the per-row table
+    double *xtab_exact = nullptr;
     double *etab = nullptr;        // packed rows of the segments that read the table
     int *toff = nullptr;           // [S]
     double *bt = nullptr;          // transposed stencil blocks (adjoint, bounded)

@@ -14,10 +14,11 @@
 //
 //   fwd      stencil rows of the segment (reference grouping), then the local
 //            forward recurrence with zero incoming state, in registers
-//   chainF   one thread per line walks the S segments: incoming states and
-//            the cyclic border unknowns
+//   chainF   every thread: its incoming state from the W segments before it
+//            (precomputed transfer products); per line, the cyclic border
+//            unknowns
 //   bwd      local backward recurrence (forward values corrected on the fly)
-//   chainB   one thread per line walks the segments backwards
+//   chainB   every thread: its incoming state from the W segments after it
 //   fin      x = local + incoming-state corrections -> df
 //
 // The adjoint kernel runs the transposed sweep first and the transposed
@@ -34,7 +35,7 @@
 namespace pado {
 
 constexpr int KMAXM = 64;  // longest segment (MAXM of pado_tables.h)
-constexpr int KCT_NF = 12; // chain coefficients per segment (CT_NF of pado_tables.h)
+constexpr int KCT_NF = 4;  // border-sum weights per segment (CT_NF of pado_tables.h)
 
 // Parameters of one launch (passed by value).
 struct KParams {
@@ -45,11 +46,13 @@ struct KParams {
     long long line_oc;
     long long stride;      // element stride along a line
     int n, nb, nbord, P;   // line length, banded rows, border rows, tile pitch
-    int S, base, rem;      // segment layout over [0, n)
+    int S;                 // segments per line
     int L;                 // lines per CTA
     int bc1, bcn;
     const double *tab;     // [nb][T_NF]
-    const double *ctab;    // [S][KCT_NF] chain coefficients
+    const double *ctab;    // [S][KCT_NF] border-sum weights G1, G2
+    const double *xtab;    // [S][W][8] transfer products Phi(s, s-d), Psi(s, s+d)
+    int W;                 // segments of coupling kept each way
     const double *bt;      // adjoint: transposed stencil blocks (bounded)
     double mb[4];
     double taps[9];        // adjoint: interior transposed taps
@@ -58,10 +61,16 @@ struct KParams {
     unsigned int_mask;     // bit s: segment s takes the register-only path
     double kc[8];          // alpha, c1, c2, gamma, d1, d2, delta
     double pu[KMAXM], pv[KMAXM], ps[KMAXM], pt[KMAXM];  // unit responses, rows 0..m-1
+    unsigned char sperm[32];  // thread slot -> segment (per-row-table segments first)
+    unsigned short sstart[33];  // segment s = rows [sstart[s], sstart[s+1])
+    unsigned char wf[32], wb[32];  // coupling window of each segment (forward, backward)
 };
 
-PADO_HD PADO_INLINE int seg_start(const KParams &kp, int s) { return s * kp.base + (s < kp.rem ? s : kp.rem); }
-PADO_HD PADO_INLINE int seg_len(const KParams &kp, int s) { return kp.base + (s < kp.rem ? 1 : 0); }
+// Segment of thread slot `slot` (= tid / L); slots >= S are idle.
+PADO_HD PADO_INLINE int slot_segment(const KParams &kp, int slot) { return slot < kp.S ? kp.sperm[slot] : slot; }
+
+PADO_HD PADO_INLINE int seg_start(const KParams &kp, int s) { return kp.sstart[s]; }
+PADO_HD PADO_INLINE int seg_len(const KParams &kp, int s) { return kp.sstart[s + 1] - kp.sstart[s]; }
 PADO_HD PADO_INLINE long long line_base(const KParams &kp, long long q)
 {
     return (q % kp.line_ia) + (q / kp.line_ia) * kp.line_oc;
@@ -74,26 +83,28 @@ struct Smem {
     double *buf4;        // [S][L][4]  forward summaries, later backward summaries
     double *buf2;        // [S][L][2]  forward incoming states, later backward ones
     double *eb;          // [L][4]     border unknowns E (0..1) and border rhs (2..3)
-    double *ctab;        // [S][KCT_NF] chain coefficients
+    double *ctab;        // [S][KCT_NF] border-sum weights
+    double *xtab;        // [S][W][8] transfer products
     double *tile;        // [L][P] or [n][L]
     const double *etab;  // packed table rows of the segments that read the table
     const int *toff;     // [S] first packed row of each segment
 };
 
 // tile_doubles: 0 (no tile), L*P ([L][P] tile) or n*L ([n][L] tile)
-PADO_HD PADO_INLINE size_t smem_doubles(int L, int S, size_t tile_doubles)
+PADO_HD PADO_INLINE size_t smem_doubles(int L, int S, int W, size_t tile_doubles)
 {
-    return (size_t)S * L * 6 + (size_t)L * 4 + (size_t)S * KCT_NF + tile_doubles;
+    return (size_t)S * L * 6 + (size_t)L * 4 + (size_t)S * KCT_NF + (size_t)S * W * 8 + tile_doubles;
 }
 
-PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S)
+PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S, int W)
 {
     Smem sm;
     sm.buf4 = base;
     sm.buf2 = sm.buf4 + (size_t)S * L * 4;
     sm.eb = sm.buf2 + (size_t)S * L * 2;
     sm.ctab = sm.eb + (size_t)L * 4;
-    sm.tile = sm.ctab + (size_t)S * KCT_NF;
+    sm.xtab = sm.ctab + (size_t)S * KCT_NF;
+    sm.tile = sm.xtab + (size_t)S * W * 8;
     sm.etab = nullptr;
     sm.toff = nullptr;
     (void)P;
@@ -188,7 +199,9 @@ PADO_HD PADO_INLINE void tile_store(const KParams &kp, const Smem &sm, long long
 }
 
 // Closure rows are rare (first/last few rows of a bounded line): evaluate
-// them out of line from memory (the tile, or global memory with a stride).
+// them out of line from memory (the tile, or global memory with a stride),
+// one function per stencil so that each holds only its own closures.
+template <int RK>
 #ifdef __CUDA_ARCH__
 __device__ __noinline__
 #else
@@ -197,7 +210,7 @@ inline
     double
     closure_row_noinline(const RhsCoef *rc, const double *line, long long stride, int n, int row, int bc1, int bcn)
 {
-    return rhs_closure_row(rc->rk, rc->c, line, stride, n, row, bc1, bcn);
+    return rhs_closure_row(RK, rc->c, line, stride, n, row, bc1, bcn);
 }
 
 // Transposed stencil at one column j of a bounded line from explicit blocks.
@@ -287,11 +300,24 @@ struct LineKernel {
             z2 = z1;
             z1 = z;
         }
+        summarize_fwd<false>(kp, sm, l, s, z1, z2, 0.0, 0.0);
+    }
+
+    // forward summary of segment s: end values y = (z1, z2) and, for a cyclic
+    // line, its share of the border sums (local sums + G_s . y)
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE void summarize_fwd(const KParams &kp, const Smem &sm, int l, int s, double z1,
+                                                  double z2, double s1, double s2)
+    {
         double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
         o[0] = z1;
         o[1] = z2;
-        o[2] = 0.0;
-        o[3] = 0.0;
+        if (CYC) {
+            const double *g = (STAGED ? sm.ctab : kp.ctab) + (size_t)s * KCT_NF;
+            const Dbl2 g1 = tld2<STAGED>(g), g2 = tld2<STAGED>(g + 2);
+            o[2] = s1 + g1.x * z1 + g1.y * z2;
+            o[3] = s2 + g2.x * z1 + g2.y * z2;
+        }
     }
 
     // ---- constant-coefficient interior segment: backward sweep -------------
@@ -360,13 +386,13 @@ struct LineKernel {
             const bool first = !PER && s == 0, last = !PER && s == kp.S - 1;
             if (first || last) {
                 for (int k = 0; k < cr; ++k) {
-                    if (live && first) cv[k] = closure_row_noinline(&kp.rc, gline, gs, n, k, kp.bc1, kp.bcn);
+                    if (live && first) cv[k] = closure_row_noinline<RK>(&kp.rc, gline, gs, n, k, kp.bc1, kp.bcn);
                 }
             }
             double cl[4] = {0.0, 0.0, 0.0, 0.0};
             if (last) {
                 for (int k = 0; k < cr; ++k)
-                    if (live) cl[k] = closure_row_noinline(&kp.rc, gline, gs, n, n - cr + k, kp.bc1, kp.bcn);
+                    if (live) cl[k] = closure_row_noinline<RK>(&kp.rc, gline, gs, n, n - cr + k, kp.bc1, kp.bcn);
             }
             // window rows a-4 .. a+len+3, all loads issued up front; the
             // stencil result of row t overwrites R.r[t], the oldest window entry
@@ -397,32 +423,42 @@ struct LineKernel {
             for (int t = 0; t < M; ++t)
                 if (t < len) R.r[t] = live ? gline[(long long)(a + t) * gs] : 0.0;
         }
-        // local forward sweep with zero incoming state
+        // local forward sweep with zero incoming state; the coefficients of
+        // eight rows are read before their recurrence steps
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
         const double *tb = seg_table(kp, sm, s, a);
+        if (lenb > 0) {
 #pragma unroll
-        for (int t = 0; t < M; ++t) {
-            if (t < lenb) {
-                const double *tr = tb + (size_t)t * T_NF;
-                const Dbl2 cc = tld2<STAGED>(tr + T_C1);
-                const Dbl2 ak = (HAS_ALPHA || CYC) ? tld2<STAGED>(tr + T_ALPHA) : Dbl2{1.0, 0.0};
-                double z = HAS_ALPHA ? ak.x * R.r[t] : R.r[t];
-                if (ORDER2) z -= cc.y * z2;
-                z -= cc.x * z1;
-                R.r[t] = z;
-                if (CYC) {
-                    s1 += ak.y * z;
-                    if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
+            for (int c0 = 0; c0 < M; c0 += 8) {
+                Dbl2 cc[8], ak[8];
+                double k2[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int tt = c0 + u < lenb ? c0 + u : lenb - 1;
+                    const double *tr = tb + (size_t)tt * T_NF;
+                    cc[u] = tld2<STAGED>(tr + T_C1);
+                    ak[u] = (HAS_ALPHA || CYC) ? tld2<STAGED>(tr + T_ALPHA) : Dbl2{1.0, 0.0};
+                    k2[u] = (CYC && ORDER2) ? tld<STAGED>(tr + T_K2) : 0.0;
                 }
-                z2 = z1;
-                z1 = z;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int t = c0 + u;
+                    if (t < lenb) {
+                        double z = HAS_ALPHA ? ak[u].x * R.r[t] : R.r[t];
+                        if (ORDER2) z -= cc[u].y * z2;
+                        z -= cc[u].x * z1;
+                        R.r[t] = z;
+                        if (CYC) {
+                            s1 += ak[u].y * z;
+                            if (ORDER2) s2 += k2[u] * z;
+                        }
+                        z2 = z1;
+                        z1 = z;
+                    }
+                }
             }
         }
-        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
-        o[0] = z1;  // z at the last banded row of the segment
-        o[1] = z2;  // and the one before
-        o[2] = s1;
-        o[3] = s2;
+        summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, s1, s2);
         if (CYC && s == kp.S - 1) {
             // border rows' right-hand sides (the last nbord rows of the line)
             double rb0 = 0.0, rb1 = 0.0;
@@ -437,46 +473,33 @@ struct LineKernel {
     }
 
     // ---- phase chainF: forward incoming states + border ------------------
-    // One thread per line walks the segments; the summaries and coefficients
-    // of four segments are read before any state is written, so the shared
-    // memory latency is paid once per four segments.
-    static PADO_HD PADO_INLINE void chain_fwd(const KParams &kp, const Smem &sm, int l)
+    // Every thread sums the transfers of the wf[s] segments before its own
+    // (no serial walk over the segments); the thread of segment 0, whose
+    // incoming state is zero, adds up the border sums of its line.
+    static PADO_HD PADO_INLINE void chain_fwd(const KParams &kp, const Smem &sm, int l, int s)
     {
-        double P1 = 0.0, P2 = 0.0, sg1 = 0.0, sg2 = 0.0;
-        const int S = kp.S, L = kp.L;
-        for (int s0 = 0; s0 < S; s0 += 4) {
-            double zl[4], zl2[4], sa[4], sb[4], c[4][8];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int s = s0 + j < S ? s0 + j : S - 1;
-                const double *in4 = sm.buf4 + ((size_t)s * L + l) * 4;
-                const double *ct = sm.ctab + (size_t)s * KCT_NF;
-                zl[j] = in4[0];
-                zl2[j] = in4[1];
-                sa[j] = CYC ? in4[2] : 0.0;
-                sb[j] = CYC ? in4[3] : 0.0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) c[j][k] = (CYC || k < 4) ? ct[k] : 0.0;
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int s = s0 + j;
-                if (s < S) {
-                    double *st = sm.buf2 + ((size_t)s * L + l) * 2;
-                    st[0] = P1;
-                    st[1] = P2;
-                    if (CYC) {
-                        sg1 += sa[j] + P1 * c[j][4] + P2 * c[j][5];
-                        sg2 += sb[j] + P1 * c[j][6] + P2 * c[j][7];
-                    }
-                    const double n1 = zl[j] + P1 * c[j][0] + P2 * c[j][1];
-                    const double n2 = zl2[j] + P1 * c[j][2] + P2 * c[j][3];
-                    P1 = n1;
-                    P2 = n2;
-                }
+        const int L = kp.L, W = kp.W, wf = kp.wf[s];
+        double P1 = 0.0, P2 = 0.0;
+        const double *xt = sm.xtab + (size_t)s * W * 8;
+        for (int d = 1; d <= wf; ++d) {
+            {
+                const double *y = sm.buf4 + ((size_t)(s - d) * L + l) * 4;
+                const double *ph = xt + (size_t)(d - 1) * 8;
+                const double y0 = y[0], y1 = y[1];
+                P1 += ph[0] * y0 + ph[1] * y1;
+                P2 += ph[2] * y0 + ph[3] * y1;
             }
         }
-        if (CYC) {
+        double *st = sm.buf2 + ((size_t)s * L + l) * 2;
+        st[0] = P1;
+        st[1] = P2;
+        if (CYC && s == 0) {
+            double sg1 = 0.0, sg2 = 0.0;
+            for (int j = 0; j < kp.S; ++j) {
+                const double *c = sm.buf4 + ((size_t)j * L + l) * 4;
+                sg1 += c[2];
+                sg2 += c[3];
+            }
             double *eb = sm.eb + (size_t)l * 4;
             const double u0 = eb[2] - sg1, u1 = eb[3] - sg2;
             if (kp.nbord == 1) {
@@ -509,25 +532,38 @@ struct LineKernel {
         }
         const double *tb = seg_table(kp, sm, s, a);
         double x1 = 0.0, x2 = 0.0;
+        if (lenb > 0) {
 #pragma unroll
-        for (int t = M - 1; t >= 0; --t) {
-            if (t < lenb) {
-                const double *tr = tb + (size_t)t * T_NF;
-                const Dbl2 uv = tld2<STAGED>(tr + T_U);
-                const Dbl2 gd = tld2<STAGED>(tr + T_GAMMA);
-                const Dbl2 de = tld2<STAGED>(tr + T_D2);
-                double z = R.r[t] + P1 * uv.x;
-                if (ORDER2) z += P2 * uv.y;
-                double x = gd.x * z;
-                if (CYC) {
-                    x -= de.y * E1;
-                    if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
+            for (int c0 = M - 4; c0 >= 0; c0 -= 4) {
+                Dbl2 uv[4], gd[4], de[4];
+                double e2[4];
+#pragma unroll
+                for (int u = 3; u >= 0; --u) {
+                    const int tt = c0 + u < lenb ? c0 + u : lenb - 1;
+                    const double *tr = tb + (size_t)tt * T_NF;
+                    uv[u] = tld2<STAGED>(tr + T_U);
+                    gd[u] = tld2<STAGED>(tr + T_GAMMA);
+                    de[u] = tld2<STAGED>(tr + T_D2);
+                    e2[u] = (CYC && ORDER2) ? tld<STAGED>(tr + T_E2) : 0.0;
                 }
-                if (ORDER2) x -= de.x * x2;
-                x -= gd.y * x1;
-                R.r[t] = x;
-                x2 = x1;
-                x1 = x;
+#pragma unroll
+                for (int u = 3; u >= 0; --u) {
+                    const int t = c0 + u;
+                    if (t < lenb) {
+                        double z = R.r[t] + P1 * uv[u].x;
+                        if (ORDER2) z += P2 * uv[u].y;
+                        double x = gd[u].x * z;
+                        if (CYC) {
+                            x -= de[u].y * E1;
+                            if (ORDER2) x -= e2[u] * E2;
+                        }
+                        if (ORDER2) x -= de[u].x * x2;
+                        x -= gd[u].y * x1;
+                        R.r[t] = x;
+                        x2 = x1;
+                        x1 = x;
+                    }
+                }
             }
         }
         double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
@@ -536,36 +572,23 @@ struct LineKernel {
     }
 
     // ---- phase chainB: backward incoming states ---------------------------
-    static PADO_HD PADO_INLINE void chain_bwd(const KParams &kp, const Smem &sm, int l)
+    static PADO_HD PADO_INLINE void chain_bwd(const KParams &kp, const Smem &sm, int l, int s)
     {
+        const int L = kp.L, W = kp.W, wb = kp.wb[s];
         double Q1 = 0.0, Q2 = 0.0;
-        const int S = kp.S, L = kp.L;
-        for (int s0 = S - 1; s0 >= 0; s0 -= 4) {
-            double x0[4], x1[4], c[4][4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int s = s0 - j >= 0 ? s0 - j : 0;
-                const double *in4 = sm.buf4 + ((size_t)s * L + l) * 4;
-                const double *ct = sm.ctab + (size_t)s * KCT_NF + 8;
-                x0[j] = in4[0];
-                x1[j] = in4[1];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) c[j][k] = ct[k];
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int s = s0 - j;
-                if (s >= 0) {
-                    double *st = sm.buf2 + ((size_t)s * L + l) * 2;
-                    st[0] = Q1;
-                    st[1] = Q2;
-                    const double n1 = x0[j] + Q1 * c[j][0] + Q2 * c[j][1];
-                    const double n2 = x1[j] + Q1 * c[j][2] + Q2 * c[j][3];
-                    Q1 = n1;
-                    Q2 = n2;
-                }
+        const double *xt = sm.xtab + (size_t)s * W * 8 + 4;
+        for (int d = 1; d <= wb; ++d) {
+            {
+                const double *w = sm.buf4 + ((size_t)(s + d) * L + l) * 4;
+                const double *ps_ = xt + (size_t)(d - 1) * 8;
+                const double w0 = w[0], w1 = w[1];
+                Q1 += ps_[0] * w0 + ps_[1] * w1;
+                Q2 += ps_[2] * w0 + ps_[3] * w1;
             }
         }
+        double *st = sm.buf2 + ((size_t)s * L + l) * 2;
+        st[0] = Q1;
+        st[1] = Q2;
     }
 
     // ---- phase fin: corrected values -> the line's output -----------------
@@ -681,6 +704,7 @@ PADO_HD PADO_INLINE LineIO tile_line_io(const KParams &kp, const Smem &sm, int l
 PADO_HD PADO_INLINE void stage_chain_table(const KParams &kp, const Smem &sm, int tid, int nthreads)
 {
     for (int i = tid; i < kp.S * KCT_NF; i += nthreads) sm.ctab[i] = kp.ctab[i];
+    for (int i = tid; i < kp.S * kp.W * 8; i += nthreads) sm.xtab[i] = kp.xtab[i];
 }
 
 // One tile of kp.L lines on a CTA of nthreads threads (nthreads >= L*S;
@@ -690,17 +714,17 @@ PADO_HD PADO_INLINE void tile_phase(int phase, const KParams &kp, const Smem &sm
                                     int nthreads)
 {
     using K = LineKernel<RK, PER, ADJ, M, IN>;
-    const int l = tid % kp.L, s = tid / kp.L;
-    const bool active = s < kp.S;
+    const int l = tid % kp.L, slot = tid / kp.L, s = slot_segment(kp, slot);
+    const bool active = slot < kp.S;
     switch (phase) {
     case PH_LOAD: tile_load(kp, sm, q0, tid, nthreads); break;
     case PH_FWD:
         stage_chain_table(kp, sm, tid, nthreads);
         if (active) K::template fwd<false>(kp, sm, R, l, s, tile_line_io<ADJ, IN>(kp, sm, l, q0));
         break;
-    case PH_CHAINF: if (s == 0) K::chain_fwd(kp, sm, l); break;
+    case PH_CHAINF: if (active) K::chain_fwd(kp, sm, l, s); break;
     case PH_BWD: if (active) K::template bwd<false>(kp, sm, R, l, s); break;
-    case PH_CHAINB: if (s == 0) K::chain_bwd(kp, sm, l); break;
+    case PH_CHAINB: if (active) K::chain_bwd(kp, sm, l, s); break;
     case PH_FIN: if (active) K::template fin<false>(kp, sm, R, l, s, tile_line_io<ADJ, IN>(kp, sm, l, q0)); break;
     case PH_ADJ_STENCIL: if (active) K::adj_stencil(kp, sm, R, l, s); break;
     case PH_ADJ_OUT:
@@ -821,7 +845,7 @@ template <int RK, bool PER, bool ADJ, int M, int IN>
 __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line_kernel(const KParams kp)
 {
     extern __shared__ double smem_raw[];
-    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S);
+    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S, kp.W);
     run_tile<RK, PER, ADJ, M, IN>(kp, sm, (long long)blockIdx.x * kp.L);
 }
 
@@ -834,10 +858,10 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
 {
     extern __shared__ double smem_raw[];
     using K = LineKernel<RK, PER, false, M, IN>;
-    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S);
+    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S, kp.W);
     const int tid = threadIdx.x, nthreads = blockDim.x;
-    const int l = tid % kp.L, s = tid / kp.L;
-    const bool active = s < kp.S;
+    const int l = tid % kp.L, slot = tid / kp.L, s = slot_segment(kp, slot);
+    const bool active = slot < kp.S;
     const long long ntiles = (kp.nlines + kp.L - 1) / kp.L;
     Regs<M> R;
     long long t = blockIdx.x;
@@ -853,11 +877,11 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
         __syncthreads();
         if (t + gridDim.x < ntiles) tile_prefetch<IN>(kp, sm, (t + gridDim.x) * kp.L, tid, nthreads);
         copy_async_commit();
-        if (s == 0) K::chain_fwd(kp, sm, l);
+        if (active) K::chain_fwd(kp, sm, l, s);
         __syncthreads();
         if (active) K::template bwd<false>(kp, sm, R, l, s);
         __syncthreads();
-        if (s == 0) K::chain_bwd(kp, sm, l);
+        if (active) K::chain_bwd(kp, sm, l, s);
         __syncthreads();
         // results go straight to global memory (the tile already holds the next input)
         LineIO out = io;
@@ -872,7 +896,7 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
 template <int RK, bool PER, bool ADJ, int M, int IN>
 inline void emulate_tile(const KParams &kp, double *smem, long long q0, int nthreads)
 {
-    const Smem sm = carve(smem, kp.L, kp.P, kp.S);
+    const Smem sm = carve(smem, kp.L, kp.P, kp.S, kp.W);
     Regs<M> *R = new Regs<M>[nthreads];
     if (IN == IN_ROWS)
         for (int tid = 0; tid < nthreads; ++tid) tile_prefetch<IN_ROWS>(kp, sm, q0, tid, nthreads);

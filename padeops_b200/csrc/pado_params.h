@@ -12,6 +12,8 @@ namespace pado {
 
 static_assert(KMAXM == MAXM && KCT_NF == CT_NF, "kernel and table builder disagree on the table shapes");
 
+inline void set_chain(KParams &kp, const ChainTables &ch);
+
 inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn)
 {
     kp.n = n;
@@ -19,8 +21,7 @@ inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn
     kp.nbord = ot.nbord;
     kp.P = (n % 2 == 0) ? n + 1 : n;
     kp.S = ot.lay.S;
-    kp.base = ot.lay.base;
-    kp.rem = ot.lay.rem;
+    for (int i = 0; i < 33; ++i) kp.sstart[i] = (unsigned short)(i <= ot.lay.S ? ot.lay.st[i] : n);
     kp.bc1 = bc1;
     kp.bcn = bcn;
     std::memcpy(kp.mb, ot.mb, sizeof(kp.mb));
@@ -33,6 +34,17 @@ inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn
     std::memcpy(kp.pv, in.pv, sizeof(kp.pv));
     std::memcpy(kp.ps, in.ps, sizeof(kp.ps));
     std::memcpy(kp.pt, in.pt, sizeof(kp.pt));
+    std::memcpy(kp.sperm, ot.sperm, sizeof(kp.sperm));
+    set_chain(kp, ot.chain);
+}
+
+// Coupling window of the chain tables in use (the table pointers are set by
+// the caller).
+inline void set_chain(KParams &kp, const ChainTables &ch)
+{
+    kp.W = ch.W;
+    std::memcpy(kp.wf, ch.wf, sizeof(kp.wf));
+    std::memcpy(kp.wb, ch.wb, sizeof(kp.wb));
 }
 
 // Field geometry of the line family along `axis` of an (n1, n2, n3) field

@@ -1,0 +1,254 @@
+// pado_resident.cuh -- per-thread phases of the tile-resident sweep used by
+// the streaming kernel: the tile of lines stays in shared memory and every
+// pass works on it in place, so a thread keeps only a 9-row stencil window
+// and a few states in registers (instead of its whole segment), and several
+// CTAs of many threads fit on one SM to hide the latency of the serial
+// recurrences.
+//
+// Thread (l, s) owns rows [a, a + len) of line l; row r of the line is
+// line[r * rs].  Per tile:
+//   prep    the 4 rows before and after the segment (the neighbours' rows,
+//           read before anyone overwrites them) and the closure rows of a
+//           bounded line
+//   fwd     stencil + local forward sweep; z overwrites f row by row
+//   chainF  incoming forward states (LineKernel::chain_fwd)
+//   bwd     local backward sweep; x overwrites z
+//   chainB  incoming backward states (LineKernel::chain_bwd)
+//   fin     corrected x -> the output line (global memory, or the tile)
+#pragma once
+
+#include "pado_kernels.cuh"
+
+namespace pado {
+
+template <int RK, bool PER, int M>
+struct ResidentLine {
+    static constexpr bool CYC = PER;
+    static constexpr bool ORDER2 = RK != RHS_CD06_D1;
+    static constexpr bool HAS_ALPHA = RK == RHS_CD06_D1 && !PER;
+    static constexpr int CR = (RK == RHS_CD06_D1 || RK == RHS_CD10_D2) ? 3 : 4;  // closure_rows(RK)
+    using LK = LineKernel<RK, PER, false, M, IN_ROWS>;
+
+    // Rows a thread needs from outside its segment, and its closure rows.
+    struct Halo {
+        double hp[4];  // rows a-4 .. a-1
+        double hn[4];  // rows a+len .. a+len+3
+        double cv[4];  // closure rows 0 .. CR-1 (first segment of a bounded line)
+        double cl[4];  // closure rows n-CR .. n-1 (last segment of a bounded line)
+    };
+
+    static PADO_HD PADO_INLINE bool fast(const KParams &kp, int s) { return (kp.int_mask >> s) & 1u; }
+    static PADO_HD PADO_INLINE int wrap(int row, int n) { return row < 0 ? row + n : (row >= n ? row - n : row); }
+    // h[j] for a runtime j in [0, 4) without indexing a register array at run
+    // time (which would move the array to local memory)
+    static PADO_HD PADO_INLINE double pick4(const double (&h)[4], int j)
+    {
+        double v = h[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (j == k) v = h[k];
+        return v;
+    }
+    static PADO_HD PADO_INLINE double row_or_zero(const double *line, long long rs, int row, int n)
+    {
+        if (PER) return line[(long long)wrap(row, n) * rs];
+        return (row >= 0 && row < n) ? line[(long long)row * rs] : 0.0;
+    }
+
+    // ---- prep: halo rows and closure rows, before any in-place write ------
+    static PADO_HD PADO_INLINE void prep(const KParams &kp, const double *line, long long rs, int s, Halo &h)
+    {
+        const int n = kp.n, a = seg_start(kp, s), len = seg_len(kp, s);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            h.hp[k] = row_or_zero(line, rs, a - 4 + k, n);
+            h.hn[k] = row_or_zero(line, rs, a + len + k, n);
+            h.cv[k] = 0.0;
+            h.cl[k] = 0.0;
+        }
+        if (!PER) {
+            if (s == 0) {
+#pragma unroll
+                for (int k = 0; k < CR; ++k) h.cv[k] = closure_row_noinline<RK>(&kp.rc, line, rs, n, k, kp.bc1, kp.bcn);
+            }
+            if (s == kp.S - 1) {
+#pragma unroll
+                for (int k = 0; k < CR; ++k)
+                    h.cl[k] = closure_row_noinline<RK>(&kp.rc, line, rs, n, n - CR + k, kp.bc1, kp.bcn);
+            }
+        }
+    }
+
+    // ---- fwd: stencil + local forward sweep, z written over f ---------------
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE void fwd(const KParams &kp, const Smem &sm, double *line, long long rs, int l, int s,
+                                        const Halo &h)
+    {
+        const int n = kp.n, nb = kp.nb;
+        const int a = seg_start(kp, s), len = seg_len(kp, s);
+        const int lenb = (a + len <= nb) ? len : nb - a;
+        double *p = line + (long long)a * rs;
+        double w[9];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w[k] = h.hp[k];
+        double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
+        if (fast(kp, s)) {
+            // len == M, every window row inside the line
+#pragma unroll
+            for (int k = 0; k < 5; ++k) w[4 + k] = p[(long long)k * rs];
+            const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
+#pragma unroll
+            for (int t = 0; t < M; ++t) {
+                double z = rhs_interior(RK, PER, kp.rc.c, w);
+                if (HAS_ALPHA) z *= al;
+                if (ORDER2) z -= c2 * z2;
+                z -= c1 * z1;
+                p[(long long)t * rs] = z;
+                z2 = z1;
+                z1 = z;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
+                if (t + 5 < M) w[8] = p[(long long)(t + 5) * rs];
+                else if (t + 5 - M < 4) w[8] = h.hn[t + 5 - M];
+            }
+            LK::template summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, 0.0, 0.0);
+            return;
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) w[4 + k] = k < len ? p[(long long)k * rs] : pick4(h.hn, k - len);
+        const double *tb = seg_table(kp, sm, s, a);
+        const bool first = !PER && s == 0, last = !PER && s == kp.S - 1;
+        double rb0 = 0.0, rb1 = 0.0;
+        // per-row table path: a plain loop (few threads take it; unrolling
+        // it would only add cold code next to the interior path)
+#pragma unroll 1
+        for (int t = 0; t < len; ++t) {
+            double r = rhs_interior(RK, PER, kp.rc.c, w);
+            if (first && t < CR) r = pick4(h.cv, t);
+            if (last && a + t >= n - CR) r = pick4(h.cl, a + t - (n - CR));
+            if (t < lenb) {
+                const double *tr = tb + (size_t)t * T_NF;
+                const Dbl2 cc = tld2<STAGED>(tr + T_C1);
+                const Dbl2 ak = (HAS_ALPHA || CYC) ? tld2<STAGED>(tr + T_ALPHA) : Dbl2{1.0, 0.0};
+                double z = HAS_ALPHA ? ak.x * r : r;
+                if (ORDER2) z -= cc.y * z2;
+                z -= cc.x * z1;
+                p[(long long)t * rs] = z;
+                if (CYC) {
+                    s1 += ak.y * z;
+                    if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
+                }
+                z2 = z1;
+                z1 = z;
+            } else {
+                // border rows of a cyclic line: right-hand sides only
+                if (t == lenb) rb0 = r;
+                else rb1 = r;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
+            const int nx = t + 5;
+            if (nx < len) w[8] = p[(long long)nx * rs];
+            else if (nx - len < 4) w[8] = pick4(h.hn, nx - len);
+        }
+        LK::template summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, s1, s2);
+        if (CYC && s == kp.S - 1) {
+            sm.eb[(size_t)l * 4 + 2] = rb0;
+            sm.eb[(size_t)l * 4 + 3] = rb1;
+        }
+    }
+
+    // ---- bwd: local backward sweep, x written over z ------------------------
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE void bwd(const KParams &kp, const Smem &sm, double *line, long long rs, int l, int s)
+    {
+        const int nb = kp.nb;
+        const int a = seg_start(kp, s), len = seg_len(kp, s);
+        const int lenb = (a + len <= nb) ? len : nb - a;
+        double *p = line + (long long)a * rs;
+        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
+        const double P1 = st[0], P2 = st[1];
+        double x1 = 0.0, x2 = 0.0;
+        if (fast(kp, s)) {
+            const double ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
+#pragma unroll
+            for (int t = M - 1; t >= 0; --t) {
+                double z = p[(long long)t * rs] + P1 * kp.pu[t];
+                if (ORDER2) z += P2 * kp.pv[t];
+                double x = ga * z;
+                if (ORDER2) x -= d2 * x2;
+                x -= d1 * x1;
+                p[(long long)t * rs] = x;
+                x2 = x1;
+                x1 = x;
+            }
+        } else {
+            double E1 = 0.0, E2 = 0.0;
+            if (CYC) {
+                E1 = sm.eb[(size_t)l * 4 + 0];
+                E2 = sm.eb[(size_t)l * 4 + 1];
+            }
+            const double *tb = seg_table(kp, sm, s, a);
+#pragma unroll 1
+            for (int t = lenb - 1; t >= 0; --t) {
+                const double *tr = tb + (size_t)t * T_NF;
+                const Dbl2 uv = tld2<STAGED>(tr + T_U);
+                const Dbl2 gd = tld2<STAGED>(tr + T_GAMMA);
+                const Dbl2 de = tld2<STAGED>(tr + T_D2);
+                double z = p[(long long)t * rs] + P1 * uv.x;
+                if (ORDER2) z += P2 * uv.y;
+                double x = gd.x * z;
+                if (CYC) {
+                    x -= de.y * E1;
+                    if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
+                }
+                if (ORDER2) x -= de.x * x2;
+                x -= gd.y * x1;
+                p[(long long)t * rs] = x;
+                x2 = x1;
+                x1 = x;
+            }
+        }
+        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
+        o[0] = x1;  // x at the segment's first row
+        o[1] = x2;  // and the second
+    }
+
+    // ---- fin: corrected x -> out (row r at out[r * os]) ----------------------
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE void fin(const KParams &kp, const Smem &sm, const double *line, long long rs, int l,
+                                        int s, double *out, long long os, bool live)
+    {
+        if (!live) return;
+        const int nb = kp.nb;
+        const int a = seg_start(kp, s), len = seg_len(kp, s);
+        const int lenb = (a + len <= nb) ? len : nb - a;
+        const double *p = line + (long long)a * rs;
+        double *q = out + (long long)a * os;
+        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
+        const double Q1 = st[0], Q2 = st[1];
+        if (fast(kp, s)) {
+#pragma unroll
+            for (int t = 0; t < M; ++t) {
+                double x = p[(long long)t * rs] + Q1 * kp.ps[t];
+                if (ORDER2) x += Q2 * kp.pt[t];
+                q[(long long)t * os] = x;
+            }
+            return;
+        }
+        const double *tb = seg_table(kp, sm, s, a);
+#pragma unroll 2
+        for (int t = 0; t < lenb; ++t) {
+            const Dbl2 stt = tld2<STAGED>(tb + (size_t)t * T_NF + T_S);
+            double x = p[(long long)t * rs] + Q1 * stt.x;
+            if (ORDER2) x += Q2 * stt.y;
+            q[(long long)t * os] = x;
+        }
+        if (CYC && s == kp.S - 1) {
+            out[(long long)nb * os] = sm.eb[(size_t)l * 4 + 0];
+            if (kp.nbord == 2) out[(long long)(nb + 1) * os] = sm.eb[(size_t)l * 4 + 1];
+        }
+    }
+};
+
+}  // namespace pado

@@ -3,15 +3,15 @@
 // (TMA), two tiles ahead, so HBM streams continuously while the CTA runs the
 // sweep of the current tile.
 //
-// One CTA per SM walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
-// through `stages` shared-memory buffers, each guarded by an mbarrier:
+// Persistent CTAs (as many per SM as fit) walk the tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... through `stages` shared-memory buffers, each
+// guarded by an mbarrier.  The sweep runs on the buffer in place
+// (pado_resident.cuh):
 //
-//   wait(full[b])  fwd (stencil + local forward sweep, reads the buffer)
-//   barrier        strided lines: buffer b is free -> issue the load of the
-//                  tile `stages` ahead into it
-//   chainF, bwd, chainB, fin (results to global memory from registers)
-//   x lines:       fin writes the buffer; bulk store of each line; then the
-//                  load `stages` ahead is issued into the buffer
+//   wait(full[b])  prep, fwd, chainF, bwd, chainB, fin (barrier-separated)
+//   strided lines: results to global memory from fin
+//   x lines:       fin writes the buffer; bulk store of each line
+//   then the load `stages` tiles ahead is issued into buffer b
 //
 // Strided lines (y, z): one 3-D tensor copy per box of {L lines, box_rows
 // rows} lands as the [row][L] tile.  Contiguous lines (x): one bulk copy per
@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "pado_kernels.cuh"
+#include "pado_resident.cuh"
 
 namespace pado {
 
@@ -55,21 +56,21 @@ struct StreamLayout {
     size_t tiles, work, etab, toff, bars, total_doubles;
 };
 
-PADO_HD PADO_INLINE StreamLayout stream_layout(int L, int S, int stages, int tile_doubles, int etab_rows)
+PADO_HD PADO_INLINE StreamLayout stream_layout(int L, int S, int W, int stages, int tile_doubles, int etab_rows)
 {
     StreamLayout o;
     o.tiles = 0;
     o.work = (size_t)stages * tile_doubles;
-    o.etab = o.work + smem_doubles(L, S, 0);
+    o.etab = o.work + smem_doubles(L, S, W, 0);
     o.toff = o.etab + (size_t)etab_rows * T_NF;
     o.bars = o.toff + (size_t)(S + 1) / 2;
     o.total_doubles = o.bars + (size_t)stages;
     return o;
 }
 
-PADO_HD PADO_INLINE size_t stream_smem_bytes(int L, int S, int stages, int tile_doubles, int etab_rows)
+PADO_HD PADO_INLINE size_t stream_smem_bytes(int L, int S, int W, int stages, int tile_doubles, int etab_rows)
 {
-    return stream_layout(L, S, stages, tile_doubles, etab_rows).total_doubles * sizeof(double) + 1024;
+    return stream_layout(L, S, W, stages, tile_doubles, etab_rows).total_doubles * sizeof(double) + 1024;
 }
 
 // Line l of strided tile t: plane p, lines x0 .. x0+L-1 of that plane.
@@ -209,15 +210,18 @@ __device__ __forceinline__ void stream_issue_load(const StreamParams &sp, double
 }
 
 template <int RK, bool PER, int M, bool XL>
-__global__ void __launch_bounds__(256, 1) stream_kernel(const __grid_constant__ StreamParams sp)
+__global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ StreamParams sp)
 {
-    using K = LineKernel<RK, PER, false, M, XL ? IN_LINES : IN_ROWS>;
+    using K = LineKernel<RK, PER, false, M, IN_ROWS>;
+    using RL = ResidentLine<RK, PER, M>;
     extern __shared__ double smem_raw[];
-    double *base = reinterpret_cast<double *>((reinterpret_cast<size_t>(smem_raw) + 1023) & ~(size_t)1023);
+    // 1024-byte aligned base, by pointer arithmetic on the shared array so
+    // that the compiler keeps every access in the shared address space
+    double *base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u) / sizeof(double);
     const KParams &kp = sp.kp;
     const int L = kp.L, S = kp.S;
-    const StreamLayout lay = stream_layout(L, S, sp.stages, sp.tile_doubles, sp.etab_rows);
-    Smem sm = carve(base + lay.work, L, kp.P, S);
+    const StreamLayout lay = stream_layout(L, S, kp.W, sp.stages, sp.tile_doubles, sp.etab_rows);
+    Smem sm = carve(base + lay.work, L, kp.P, S, kp.W);
     double *etab = base + lay.etab;
     int *toff = reinterpret_cast<int *>(base + lay.toff);
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + lay.bars);
@@ -225,17 +229,19 @@ __global__ void __launch_bounds__(256, 1) stream_kernel(const __grid_constant__ 
     sm.toff = toff;
 
     const int tid = threadIdx.x, nthreads = blockDim.x;
-    const int l = tid % L, s = tid / L;
-    const bool active = s < S;
+    const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
+    const bool active = slot < S;
     const long long G = gridDim.x;
     const long long t_first = blockIdx.x;
     const int stages = sp.stages;
+    // row r of line l in a stage buffer: [row][L] (y, z) or [L][P] (x)
+    const long long rs = XL ? 1 : L, ls = XL ? kp.P : 1;
 
     if (tid == 0) {
         for (int b = 0; b < stages; ++b) mbar_init(&bars[b], 1);
         mbar_fence_init();
     }
-    for (int i = tid; i < S * KCT_NF; i += nthreads) sm.ctab[i] = kp.ctab[i];
+    stage_chain_table(kp, sm, tid, nthreads);
     for (int i = tid; i < sp.etab_rows * T_NF; i += nthreads) etab[i] = __ldg(sp.etab + i);
     for (int i = tid; i < S; i += nthreads) toff[i] = __ldg(sp.toff + i);
     __syncthreads();
@@ -246,7 +252,6 @@ __global__ void __launch_bounds__(256, 1) stream_kernel(const __grid_constant__ 
         }
     }
 
-    Regs<M> R;
     long long k = 0;
     for (long long t = t_first; t < sp.ntiles; t += G, ++k) {
         const int b = (int)(k % stages);
@@ -266,18 +271,21 @@ __global__ void __launch_bounds__(256, 1) stream_kernel(const __grid_constant__ 
             return;
         }
         sm.tile = base + (size_t)b * sp.tile_doubles;
+        double *line = sm.tile + l * ls;
         const LineIO io = stream_line_io(sp, sm, l, t);
-        if (active) K::template fwd<true>(kp, sm, R, l, s, io);
+        typename RL::Halo h;
+        if (active) RL::prep(kp, line, rs, s, h);
         __syncthreads();
+        if (active) RL::template fwd<true>(kp, sm, line, rs, l, s, h);
+        __syncthreads();
+        if (active) K::chain_fwd(kp, sm, l, s);
+        __syncthreads();
+        if (active) RL::template bwd<true>(kp, sm, line, rs, l, s);
+        __syncthreads();
+        if (active) K::chain_bwd(kp, sm, l, s);
+        __syncthreads();
+        if (active) RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live);
         const long long tn = t + (long long)stages * G;  // tile for this buffer next
-        if (!XL && tid == 0 && tn < sp.ntiles) stream_issue_load(sp, sm.tile, &bars[b], tn);
-        if (s == 0) K::chain_fwd(kp, sm, l);
-        __syncthreads();
-        if (active) K::template bwd<true>(kp, sm, R, l, s);
-        __syncthreads();
-        if (s == 0) K::chain_bwd(kp, sm, l);
-        __syncthreads();
-        if (active) K::template fin<true>(kp, sm, R, l, s, io);
         if (XL) {
             // each line's results -> global memory, then the buffer takes the next load
             fence_proxy_async();
@@ -288,9 +296,9 @@ __global__ void __launch_bounds__(256, 1) stream_kernel(const __grid_constant__ 
                 bulk_commit();
                 bulk_wait_read();
             }
-            __syncthreads();
-            if (tid == 0 && tn < sp.ntiles) stream_issue_load(sp, sm.tile, &bars[b], tn);
         }
+        __syncthreads();
+        if (tid == 0 && tn < sp.ntiles) stream_issue_load(sp, sm.tile, &bars[b], tn);
     }
     if (XL) bulk_wait_all();
 }
@@ -301,22 +309,24 @@ __global__ void __launch_bounds__(256, 1) stream_kernel(const __grid_constant__ 
 template <int RK, bool PER, int M, bool XL>
 inline void emulate_stream(const StreamParams &sp, int nthreads)
 {
-    using K = LineKernel<RK, PER, false, M, XL ? IN_LINES : IN_ROWS>;
+    using K = LineKernel<RK, PER, false, M, IN_ROWS>;
+    using RL = ResidentLine<RK, PER, M>;
     const KParams &kp = sp.kp;
     const int L = kp.L, S = kp.S;
-    const StreamLayout lay = stream_layout(L, S, 1, sp.tile_doubles, sp.etab_rows);
+    const StreamLayout lay = stream_layout(L, S, kp.W, 1, sp.tile_doubles, sp.etab_rows);
     std::vector<double> mem(lay.total_doubles, 0.0);
     double *base = mem.data();
-    Smem sm = carve(base + lay.work, L, kp.P, S);
+    Smem sm = carve(base + lay.work, L, kp.P, S, kp.W);
     double *etab = base + lay.etab;
     int *toff = reinterpret_cast<int *>(base + lay.toff);
-    for (int i = 0; i < S * KCT_NF; ++i) sm.ctab[i] = kp.ctab[i];
+    stage_chain_table(kp, sm, 0, 1);
     for (int i = 0; i < sp.etab_rows * T_NF; ++i) etab[i] = sp.etab[i];
     for (int i = 0; i < S; ++i) toff[i] = sp.toff[i];
     sm.etab = etab;
     sm.toff = toff;
     sm.tile = base;
-    std::vector<Regs<M>> R(nthreads);
+    const long long rs = XL ? 1 : L, ls = XL ? kp.P : 1;
+    std::vector<typename RL::Halo> H(nthreads);
     for (long long t = 0; t < sp.ntiles; ++t) {
         long long x0, p;
         stream_tile_origin(sp, t, &x0, &p);
@@ -330,17 +340,19 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
                 else sm.tile[(size_t)r * L + ll] = kp.in[x0 + ll + p * sp.pstride + (long long)r * kp.stride];
             }
         }
-        for (int ph = 0; ph < 5; ++ph) {
+        for (int ph = 0; ph < 6; ++ph) {
             for (int tid = 0; tid < nthreads; ++tid) {
-                const int l = tid % L, s = tid / L;
-                const bool active = s < S;
+                const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
+                if (slot >= S) continue;
+                double *line = sm.tile + l * ls;
                 const LineIO io = stream_line_io(sp, sm, l, t);
                 switch (ph) {
-                case 0: if (active) K::template fwd<true>(kp, sm, R[tid], l, s, io); break;
-                case 1: if (s == 0) K::chain_fwd(kp, sm, l); break;
-                case 2: if (active) K::template bwd<true>(kp, sm, R[tid], l, s); break;
-                case 3: if (s == 0) K::chain_bwd(kp, sm, l); break;
-                default: if (active) K::template fin<true>(kp, sm, R[tid], l, s, io); break;
+                case 0: RL::prep(kp, line, rs, s, H[tid]); break;
+                case 1: RL::template fwd<true>(kp, sm, line, rs, l, s, H[tid]); break;
+                case 2: K::chain_fwd(kp, sm, l, s); break;
+                case 3: RL::template bwd<true>(kp, sm, line, rs, l, s); break;
+                case 4: K::chain_bwd(kp, sm, l, s); break;
+                default: RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live); break;
                 }
             }
         }

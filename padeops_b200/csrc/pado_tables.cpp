@@ -2,6 +2,7 @@
 #include "pado_tables.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 
@@ -384,15 +385,78 @@ Sweep adjoint_sweep(const Sweep &p)
     return a;
 }
 
-Layout make_layout(int n, int m_max)
+Layout make_layout(int n, int m, int i0, int i1)
 {
     Layout L;
     L.n = n;
-    L.S = (n + m_max - 1) / m_max;
-    if (L.S < 1) L.S = 1;
-    L.base = n / L.S;
-    L.rem = n % L.S;
+    auto uniform = [&](int S) {
+        L.S = std::max(1, std::min(S, n));
+        L.st.assign(L.S + 1, 0);
+        for (int s = 0; s <= L.S; ++s) L.st[s] = (int)((long long)n * s / L.S);
+    };
+    const int A = std::max(i0, HALO), B = std::min(i1, n - HALO);
+    int k = (i0 < i1 && B > A) ? (B - A) / m : 0;
+    if (k < 1 || m < 8) {
+        uniform((n + m - 1) / m);
+        return L;
+    }
+    // pieces of at most e rows, at least 4, on each side of the interior block
+    int e = std::max(4, (m + 2) / 3);
+    auto pieces = [](int rows, int e_) { return rows <= 0 ? 0 : (rows + e_ - 1) / e_; };
+    for (;;) {
+        const int right = n - (A + k * m);
+        const int S = k + pieces(A, e) + pieces(right, e);
+        if (S <= MAX_SEGMENTS) break;
+        if (e < m) ++e;
+        else if (k > 1) --k;
+        else {
+            uniform((n + m - 1) / m);
+            return L;
+        }
+    }
+    L.st.clear();
+    auto cut = [&](int lo, int hi) {  // near-equal pieces of [lo, hi)
+        const int np = pieces(hi - lo, e);
+        for (int j = 0; j < np; ++j) L.st.push_back(lo + (int)((long long)(hi - lo) * j / np));
+    };
+    cut(0, A);
+    for (int j = 0; j < k; ++j) L.st.push_back(A + j * m);
+    cut(A + k * m, n);
+    L.st.push_back(n);
+    L.S = (int)L.st.size() - 1;
     return L;
+}
+
+void interior_range(const Sweep &sw, int *i0, int *i1)
+{
+    *i0 = *i1 = 0;
+    const int nb = sw.nb;
+    if (nb < 16) return;
+    const int mid = nb / 2;
+    const double ref[7] = {sw.alpha[mid], sw.c1[mid], sw.c2[mid], sw.gamma[mid], sw.d1[mid], sw.d2[mid], sw.delta[mid]};
+    double kmax = 0.0, emax = 0.0;
+    for (int i = 0; i < nb; ++i) {
+        kmax = std::max({kmax, std::fabs(sw.k1[i]), std::fabs(sw.k2[i])});
+        emax = std::max({emax, std::fabs(sw.e1[i]), std::fabs(sw.e2[i])});
+    }
+    // a row is interior when its coefficients equal the line-centre values to
+    // 1e-14 relative (they settle to a few ulps) and its cyclic spike terms
+    // are below 1e-17 of their largest magnitude (their contribution is far
+    // below one rounding of the sums they enter)
+    auto ok = [&](int i) {
+        const double v[7] = {sw.alpha[i], sw.c1[i], sw.c2[i], sw.gamma[i], sw.d1[i], sw.d2[i], sw.delta[i]};
+        for (int k = 0; k < 7; ++k)
+            if (std::fabs(v[k] - ref[k]) > 1e-14 * std::fabs(ref[k])) return false;
+        if (std::fabs(sw.k1[i]) > 1e-17 * kmax || std::fabs(sw.k2[i]) > 1e-17 * kmax) return false;
+        if (std::fabs(sw.e1[i]) > 1e-17 * emax || std::fabs(sw.e2[i]) > 1e-17 * emax) return false;
+        return true;
+    };
+    if (!ok(mid)) return;
+    int a = mid, b = mid + 1;
+    while (a > 0 && ok(a - 1)) --a;
+    while (b < nb && ok(b)) ++b;
+    *i0 = a;
+    *i1 = b;
 }
 
 void build_device_table(const Sweep &sw, const Layout &lay, std::vector<double> &tab, std::vector<double> &segsum)
@@ -452,31 +516,11 @@ void build_device_table(const Sweep &sw, const Layout &lay, std::vector<double> 
 Interior interior_info(const Sweep &sw, const Layout &lay, int m)
 {
     Interior in;
-    const int nb = sw.nb;
-    if (nb < 16) return in;
-    const int mid = nb / 2;
+    int i0, i1;
+    interior_range(sw, &i0, &i1);
+    if (i0 >= i1) return in;
+    const int mid = sw.nb / 2;
     const double ref[7] = {sw.alpha[mid], sw.c1[mid], sw.c2[mid], sw.gamma[mid], sw.d1[mid], sw.d2[mid], sw.delta[mid]};
-    double kmax = 0.0, emax = 0.0;
-    for (int i = 0; i < nb; ++i) {
-        kmax = std::max({kmax, std::fabs(sw.k1[i]), std::fabs(sw.k2[i])});
-        emax = std::max({emax, std::fabs(sw.e1[i]), std::fabs(sw.e2[i])});
-    }
-    // a row is interior when its coefficients equal the line-centre values to
-    // 1e-14 relative (they settle to a few ulps) and its cyclic spike terms
-    // are below 1e-17 of their largest magnitude (their contribution is far
-    // below one rounding of the sums they enter)
-    auto ok = [&](int i) {
-        const double v[7] = {sw.alpha[i], sw.c1[i], sw.c2[i], sw.gamma[i], sw.d1[i], sw.d2[i], sw.delta[i]};
-        for (int k = 0; k < 7; ++k)
-            if (std::fabs(v[k] - ref[k]) > 1e-14 * std::fabs(ref[k])) return false;
-        if (std::fabs(sw.k1[i]) > 1e-17 * kmax || std::fabs(sw.k2[i]) > 1e-17 * kmax) return false;
-        if (std::fabs(sw.e1[i]) > 1e-17 * emax || std::fabs(sw.e2[i]) > 1e-17 * emax) return false;
-        return true;
-    };
-    if (!ok(mid)) return in;
-    int i0 = mid, i1 = mid + 1;
-    while (i0 > 0 && ok(i0 - 1)) --i0;
-    while (i1 < nb && ok(i1)) ++i1;
     in.i0 = i0;
     in.i1 = i1;
     for (int k = 0; k < 7; ++k) in.kc[k] = ref[k];
@@ -504,29 +548,89 @@ Interior interior_info(const Sweep &sw, const Layout &lay, int m)
     return in;
 }
 
-std::vector<double> chain_table(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay,
-                                int nb, const Interior &in, int m)
+ChainTables chain_tables(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay, int nb,
+                         const Interior &in, int m)
 {
-    std::vector<double> ct((size_t)lay.S * CT_NF, 0.0);
+    const int S = lay.S;
     auto T = [&](int i, int f) { return tab[(size_t)i * T_NF + f]; };
-    for (int s = 0; s < lay.S; ++s) {
-        double *c = &ct[(size_t)s * CT_NF];
+    // per-segment transfers
+    std::vector<std::array<double, 4>> A(S, {0, 0, 0, 0}), B(S, {0, 0, 0, 0});
+    for (int s = 0; s < S; ++s) {
         const bool fast = (in.mask >> s) & 1u;
         const int a = lay.start(s);
-        for (int k = 0; k < 4; ++k) c[4 + k] = segsum[(size_t)s * 4 + k];
-        if (s + 1 < lay.S) {
+        if (s + 1 < S) {
             const int b = lay.start(s + 1);  // segments before the last are fully banded
-            c[0] = fast ? in.pu[m - 1] : T(b - 1, T_U);
-            c[1] = fast ? in.pv[m - 1] : T(b - 1, T_V);
-            c[2] = fast ? in.pu[m - 2] : T(b - 2, T_U);
-            c[3] = fast ? in.pv[m - 2] : T(b - 2, T_V);
+            A[s] = {fast ? in.pu[m - 1] : T(b - 1, T_U), fast ? in.pv[m - 1] : T(b - 1, T_V),
+                    fast ? in.pu[m - 2] : T(b - 2, T_U), fast ? in.pv[m - 2] : T(b - 2, T_V)};
         }
         if (s > 0) {
-            c[8] = fast ? in.ps[0] : T(a, T_S);
-            c[9] = fast ? in.pt[0] : T(a, T_T);
-            c[10] = fast ? in.ps[1] : (a + 1 < nb ? T(a + 1, T_S) : 0.0);
-            c[11] = fast ? in.pt[1] : (a + 1 < nb ? T(a + 1, T_T) : 0.0);
+            B[s] = {fast ? in.ps[0] : T(a, T_S), fast ? in.pt[0] : T(a, T_T),
+                    fast ? in.ps[1] : (a + 1 < nb ? T(a + 1, T_S) : 0.0),
+                    fast ? in.pt[1] : (a + 1 < nb ? T(a + 1, T_T) : 0.0)};
         }
+    }
+    auto mul = [](const std::array<double, 4> &x, const std::array<double, 4> &y) {
+        return std::array<double, 4>{x[0] * y[0] + x[1] * y[2], x[0] * y[1] + x[1] * y[3],
+                                     x[2] * y[0] + x[3] * y[2], x[2] * y[1] + x[3] * y[3]};
+    };
+    auto norm = [](const std::array<double, 4> &x) {
+        return std::max({std::fabs(x[0]), std::fabs(x[1]), std::fabs(x[2]), std::fabs(x[3])});
+    };
+    const std::array<double, 4> I = {1, 0, 0, 1};
+    // phi[s][j], psi[s][j] for all pairs (S <= 32)
+    std::vector<std::array<double, 4>> phi((size_t)S * S, {0, 0, 0, 0}), psi((size_t)S * S, {0, 0, 0, 0});
+    for (int s = 0; s < S; ++s) {
+        std::array<double, 4> M_ = I;
+        for (int j = s - 1; j >= 0; --j) {  // Phi(s, j) = Phi(s, j+1) A_{j+1}
+            if (j < s - 1) M_ = mul(M_, A[j + 1]);
+            phi[(size_t)s * S + j] = M_;
+        }
+        M_ = I;
+        for (int j = s + 1; j < S; ++j) {  // Psi(s, j) = Psi(s, j-1) B_{j-1}
+            if (j > s + 1) M_ = mul(M_, B[j - 1]);
+            psi[(size_t)s * S + j] = M_;
+        }
+    }
+    ChainTables ct;
+    int W = 0;
+    for (int s = 0; s < S; ++s) {
+        int wf = 0, wb = 0;
+        for (int j = 0; j < S; ++j) {
+            if (j < s && norm(phi[(size_t)s * S + j]) >= XFER_DROP) wf = std::max(wf, s - j);
+            if (j > s && norm(psi[(size_t)s * S + j]) >= XFER_DROP) wb = std::max(wb, j - s);
+        }
+        ct.wf[s] = (unsigned char)wf;
+        ct.wb[s] = (unsigned char)wb;
+        W = std::max({W, wf, wb});
+    }
+    ct.W = W;
+    ct.xtab.assign((size_t)S * std::max(W, 1) * 8, 0.0);
+    for (int s = 0; s < S; ++s)
+        for (int d = 1; d <= W; ++d) {
+            double *x = &ct.xtab[((size_t)s * W + (d - 1)) * 8];
+            if (s - d >= 0) {
+                const auto &p = phi[(size_t)s * S + (s - d)];
+                if (norm(p) >= XFER_DROP) std::copy(p.begin(), p.end(), x);
+            }
+            if (s + d < S) {
+                const auto &p = psi[(size_t)s * S + (s + d)];
+                if (norm(p) >= XFER_DROP) std::copy(p.begin(), p.end(), x + 4);
+            }
+        }
+    // border-sum weights (every term kept)
+    ct.ctab.assign((size_t)S * CT_NF, 0.0);
+    for (int j = 0; j < S; ++j) {
+        double g[4] = {0, 0, 0, 0};
+        for (int t = j + 1; t < S; ++t) {
+            const auto &p = phi[(size_t)t * S + j];
+            const double k1u = segsum[(size_t)t * 4 + 0], k1v = segsum[(size_t)t * 4 + 1];
+            const double k2u = segsum[(size_t)t * 4 + 2], k2v = segsum[(size_t)t * 4 + 3];
+            g[0] += k1u * p[0] + k1v * p[2];
+            g[1] += k1u * p[1] + k1v * p[3];
+            g[2] += k2u * p[0] + k2v * p[2];
+            g[3] += k2u * p[1] + k2v * p[3];
+        }
+        std::copy(g, g + 4, &ct.ctab[(size_t)j * CT_NF]);
     }
     return ct;
 }
@@ -556,13 +660,21 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     ot.m = m;
     std::memcpy(ot.mb, sw.mb, sizeof(ot.mb));
     ot.rc = make_rhs_coef(scheme, kind, dx, periodic);
-    ot.lay = make_layout(n, m);
+    int i0, i1;
+    interior_range(sw, &i0, &i1);
+    ot.lay = make_layout(n, m, i0, i1);
     std::vector<double> segsum;
     build_device_table(sw, ot.lay, ot.tab, segsum);
     ot.interior = interior_info(sw, ot.lay, m);
-    ot.ctab = chain_table(ot.tab, segsum, ot.lay, sw.nb, ot.interior, m);
-    ot.ctab_exact = chain_table(ot.tab, segsum, ot.lay, sw.nb, Interior{}, m);
+    ot.chain = chain_tables(ot.tab, segsum, ot.lay, sw.nb, ot.interior, m);
+    ot.chain_exact = chain_tables(ot.tab, segsum, ot.lay, sw.nb, Interior{}, m);
     edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask, ot.etab, ot.toff);
+    // thread slots: segments on the per-row table first, so that a warp's
+    // segments take one path
+    int k = 0;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int s = 0; s < ot.lay.S && s < 32; ++s)
+            if ((((ot.interior.mask >> s) & 1u) != 0) == (pass == 1)) ot.sperm[k++] = (unsigned char)s;
     if (adjoint) {
         double taps[9];
         interior_taps(ot.rc, taps);

@@ -34,13 +34,23 @@ Sweep primal_sweep(int scheme, int kind, int n, int periodic, int bc1, int bcn);
 // The sweep of the transposed solve A^{-T}.
 Sweep adjoint_sweep(const Sweep &p);
 
-// Cut of [0, n) into S segments of length base+1 (first rem) or base.
+// Cut of [0, n) into S <= 32 segments, segment s = rows [st[s], st[s+1]).
 struct Layout {
-    int n = 0, S = 1, base = 0, rem = 0;
-    int start(int s) const { return s * base + (s < rem ? s : rem); }
-    int len(int s) const { return base + (s < rem ? 1 : 0); }
+    int n = 0, S = 1;
+    std::vector<int> st{0, 0};
+    int start(int s) const { return st[s]; }
+    int len(int s) const { return st[s + 1] - st[s]; }
 };
-Layout make_layout(int n, int m_max);
+// With an interior [i0, i1) (i0 < i1): as many segments of exactly m rows as
+// fit in it, and the rows before and after cut into short pieces (about m/3
+// rows: they run the per-row-table path, about three times slower per row),
+// so that every thread of a tile finishes at about the same time.  Without
+// one: ceil(n/m) segments of near-equal length.
+constexpr int MAX_SEGMENTS = 32;
+Layout make_layout(int n, int m, int i0 = 0, int i1 = 0);
+// Banded rows [i0, i1) whose coefficients have settled (see Interior);
+// i0 == i1 == 0 when there are none.
+void interior_range(const Sweep &sw, int *i0, int *i1);
 
 // Device table: T_NF doubles per banded row (TabField order) with the
 // segment responses folded in, plus 4 segment sums per segment
@@ -65,15 +75,29 @@ struct Interior {
 };
 Interior interior_info(const Sweep &sw, const Layout &lay, int m);
 
-// Chain coefficients, CT_NF per segment s:
-//   0..3   U(b-1), V(b-1), U(b-2), V(b-2): forward transfer to segment s+1
-//   4..7   k1.U, k1.V, k2.U, k2.V summed over the segment (cyclic sums)
-//   8..11  S(a), T(a), S(a+1), T(a+1): backward transfer to segment s-1
-// (a, b: first row of segment s and of segment s+1).  Constant-coefficient
-// segments take the responses of Interior.
-constexpr int CT_NF = 12;
-std::vector<double> chain_table(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay,
-                                int nb, const Interior &in, int m);
+// Inter-segment coupling.  With A_s = [[U(b-1), V(b-1)], [U(b-2), V(b-2)]]
+// the forward transfer of segment s (a, b: first rows of segments s and
+// s+1) and B_s = [[S(a), T(a)], [S(a+1), T(a+1)]] the backward one, the
+// incoming states are
+//   P_s = sum_{j<s} Phi(s,j) y_j,  Phi(s,j) = A_{s-1} ... A_{j+1}
+//   Q_s = sum_{j>s} Psi(s,j) w_j,  Psi(s,j) = B_{s+1} ... B_{j-1}
+// (y_j, w_j: the local end / first values of segment j).  The products decay
+// like the sweep's homogeneous solutions; those below XFER_DROP are dropped,
+// which bounds the window W.
+//   xtab [S][W][8]: Phi(s, s-d) (4, row-major) and Psi(s, s+d) (4), d = 1..W
+//   ctab [S][CT_NF]: G1_s, G2_s with G_s = sum_{t>s} k_t Phi(t, s), k_t the
+//                    (k.U, k.V) sums of segment t: the cyclic border sums are
+//                    sum_s (local sum_s + G_s . y_s)
+// Constant-coefficient segments take the responses of Interior.
+constexpr int CT_NF = 4;
+constexpr double XFER_DROP = 1e-20;
+struct ChainTables {
+    std::vector<double> ctab, xtab;
+    int W = 0;
+    unsigned char wf[MAX_SEGMENTS] = {0}, wb[MAX_SEGMENTS] = {0};  // per-segment windows (<= W)
+};
+ChainTables chain_tables(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay, int nb,
+                         const Interior &in, int m);
 
 // Rows of the segments that read the per-row table, packed in segment order;
 // toff[s] = first packed row of segment s (0 for constant-coefficient ones).
@@ -89,9 +113,11 @@ struct OpTables {
     Layout lay;
     RhsCoef rc{};
     Interior interior;
-    std::vector<double> tab, ctab, etab, bt;
-    std::vector<double> ctab_exact;  // chain coefficients with every segment on the per-row table
+    std::vector<double> tab, etab, bt;
+    ChainTables chain;        // coupling of the segments as the kernels run them
+    ChainTables chain_exact;  // with every segment on the per-row table
     std::vector<int> toff;
+    unsigned char sperm[32] = {0};  // thread slot -> segment: per-row-table segments first
 };
 OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, bool adjoint);
 

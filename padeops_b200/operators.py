@@ -103,6 +103,15 @@ class _Scheme:
         with prefetch, 4 = the streaming (TMA-fed) kernel."""
         check(L.lib().pado_set_kernel_variant(self.handle, variant), "set_variant")
 
+    def launch_plan(self, kind: int, axis: int, f: torch.Tensor, df: torch.Tensor, na: int, nb: int,
+                    bc1: int = 0, bcn: int = 0) -> dict:
+        """The kernel and tiling a forward apply with these arguments would use."""
+        info = (ctypes.c_int * 8)()
+        check(L.lib().pado_launch_plan(self.handle, kind, axis, ctypes.c_void_p(f.data_ptr()),
+                                       ctypes.c_void_p(df.data_ptr()), na, nb, bc1, bcn, info), "launch_plan")
+        keys = ("variant", "lines", "stages", "ctas_per_sm", "segments", "window", "threads", "smem")
+        return dict(zip(keys, list(info)))
+
     def device_status(self, clear: bool = True) -> int:
         """Status recorded by this handle's kernels (0, or PADO_E_TIMEOUT)."""
         rc = int(L.lib().pado_device_status(self.handle, 1 if clear else 0))

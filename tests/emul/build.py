@@ -9,7 +9,7 @@ OUT = os.path.join(HERE, "_build", "libpado_emul.so")
 SRCS = [os.path.join(HERE, "pado_emul.cu"), os.path.join(ROOT, "padeops_b200", "csrc", "pado_tables.cpp")]
 DEPS = SRCS + [os.path.join(ROOT, "padeops_b200", "csrc", h) for h in ("pado_kernels.cuh", "pado_common.h",
                                                                         "pado_tables.h", "pado_params.h",
-                                                                        "pado_stream.cuh")]
+                                                                        "pado_stream.cuh", "pado_resident.cuh")]
 
 
 def build() -> str:

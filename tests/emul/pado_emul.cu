@@ -20,7 +20,7 @@ static void run_all(const KParams &kp, int nthreads)
 {
     const bool strided = kp.stride != 1;
     const size_t tile = (ADJ || !strided) ? (size_t)kp.L * kp.P : (size_t)kp.n * kp.L;
-    std::vector<double> smem(smem_doubles(kp.L, kp.S, tile), 0.0);
+    std::vector<double> smem(smem_doubles(kp.L, kp.S, kp.W, tile), 0.0);
     for (long long q0 = 0; q0 < kp.nlines; q0 += kp.L) {
         if (!strided) emulate_tile<RK, PER, ADJ, M, IN_LINES>(kp, smem.data(), q0, nthreads);
         else if (ADJ) emulate_tile<RK, PER, ADJ, M, IN_GLOBAL>(kp, smem.data(), q0, nthreads);
@@ -52,7 +52,6 @@ extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, 
 {
     const OpTables ot = make_op_tables(scheme, kind, n, dx, periodic, bc1, bcn, m, adjoint != 0);
     const Layout &lay = ot.lay;
-    if ((lay.S > 1 && lay.base + (lay.rem ? 1 : 0) > m) || lay.base + 1 > m + 1) return -6;
     KParams kp{};
     fill_params(kp, ot, n, bc1, bcn);
     kp.in = f;
@@ -60,9 +59,15 @@ extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, 
     set_geometry(kp, axis, n, na, nb);
     kp.L = lines;
     kp.tab = ot.tab.data();
-    kp.ctab = fast ? ot.ctab.data() : ot.ctab_exact.data();
+    const ChainTables &ch = fast ? ot.chain : ot.chain_exact;
+    kp.ctab = ch.ctab.data();
+    kp.xtab = ch.xtab.data();
+    set_chain(kp, ch);
     kp.bt = ot.bt.empty() ? nullptr : ot.bt.data();
-    if (!fast) kp.int_mask = 0u;
+    if (!fast) {
+        kp.int_mask = 0u;
+        for (int i = 0; i < 32; ++i) kp.sperm[i] = (unsigned char)i;
+    }
     const int nthreads = lines * lay.S + extra_threads;
     switch (ot.rc.rk) {
     case RHS_CD06_D1: return pick<RHS_CD06_D1>(kp, periodic, adjoint, m, nthreads);
@@ -93,7 +98,6 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
 {
     const OpTables ot = make_op_tables(scheme, kind, n, dx, periodic, bc1, bcn, m, false);
     const Layout &lay = ot.lay;
-    if ((lay.S > 1 && lay.base + (lay.rem ? 1 : 0) > m) || lay.base + 1 > m + 1) return -6;
     StreamParams sp;
     std::memset(&sp, 0, sizeof(sp));
     KParams &kp = sp.kp;
@@ -103,7 +107,8 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
     set_geometry(kp, axis, n, na, nb);
     kp.L = lines;
     kp.tab = ot.tab.data();
-    kp.ctab = ot.ctab.data();
+    kp.ctab = ot.chain.ctab.data();
+    kp.xtab = ot.chain.xtab.data();
     const bool xl = axis == 1;
     sp.axis = axis;
     sp.stages = 1;
