@@ -140,13 +140,13 @@ EncodeTiledFn encode_tiled()
     return fn;
 }
 
-StreamFn pick_stream(int rk, bool per, int m, bool xl)
+StreamFn pick_stream(int rk, bool per, int m, bool xl, int lines)
 {
     switch (rk) {
-    case RHS_CD06_D1: return pick_stream_rk0(per, m, xl);
-    case RHS_CD10_D1: return pick_stream_rk1(per, m, xl);
-    case RHS_CD10_D2: return pick_stream_rk2(per, m, xl);
-    default: return pick_stream_rk3(per, m, xl);
+    case RHS_CD06_D1: return pick_stream_rk0(per, m, xl, lines);
+    case RHS_CD10_D1: return pick_stream_rk1(per, m, xl, lines);
+    case RHS_CD10_D2: return pick_stream_rk2(per, m, xl, lines);
+    default: return pick_stream_rk3(per, m, xl, lines);
     }
 }
 
@@ -194,11 +194,12 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     if (align_bits & 15) return false;
     if (xl ? (n % 2 != 0) : (na % 2 != 0 || na > 0x7fffffffLL || nb > 0x7fffffffLL)) return false;
     const int etab_rows = (int)(dt.host.etab.size() / T_NF);
-    StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl);
-    if (!grant_smem(fn)) return false;
     int best_warps = 0, bestL = 0, best_stages = 0, best_ctas = 0;
     for (int L : {16, 32, 8}) {
         if (L * S > 384) continue;  // the kernel is built for 384 threads, two CTAs per SM
+        if (!xl && L == 32) continue;  // strided-line kernels exist for 8 and 16 lines per tile
+        StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L);
+        if (!grant_smem(fn)) continue;
         for (int stages : {2, 1}) {
             const int tile_doubles = stream_tile_doubles(xl, n, L);
             const size_t bytes = stream_smem_bytes(L, S, kp0.W, stages, tile_doubles, etab_rows);
@@ -270,7 +271,7 @@ int sm_count()
 
 int launch_stream(pado_op_s *op, const StreamParams &sp, int threads, size_t smem, int ctas_per_sm, cudaStream_t st)
 {
-    StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1);
+    StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1, sp.kp.L);
     const long long grid = std::min<long long>(sp.ntiles, (long long)ctas_per_sm * sm_count());
     if (grid < 1) return PADO_OK;
     fn<<<(unsigned)grid, threads, smem, st>>>(sp);
@@ -315,6 +316,7 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
     if (no_fast) {
         // every segment on the per-row table (kernels built for another segment length)
         kp.int_mask = 0;
+        kp.spk_mask = 0;
         kp.ctab = dt.ctab_exact;
         kp.xtab = dt.xtab_exact;
         set_chain(kp, dt.host.chain_exact);

@@ -30,23 +30,29 @@ KernelFn pick_m(int m, bool adj, bool contiguous, int variant)
     }
 }
 
-template <bool PER, bool XL>
+template <bool PER, bool XL, int LT>
 StreamFn pick_stream_m(int m)
 {
     constexpr int RK = 2;
     switch (m) {
-    case 16: return stream_kernel<RK, PER, 16, XL>;
-    case 32: return stream_kernel<RK, PER, 32, XL>;
-    default: return stream_kernel<RK, PER, 64, XL>;
+    case 16: return stream_kernel<RK, PER, 16, XL, LT>;
+    case 32: return stream_kernel<RK, PER, 32, XL, LT>;
+    default: return stream_kernel<RK, PER, 64, XL, LT>;
     }
+}
+
+template <bool PER>
+StreamFn pick_stream_l(int m, bool xl, int lines)
+{
+    if (xl) return pick_stream_m<PER, true, 0>(m);
+    return lines == 8 ? pick_stream_m<PER, false, 8>(m) : pick_stream_m<PER, false, 16>(m);
 }
 
 }  // namespace
 
-StreamFn pick_stream_rk2(bool per, int m, bool xl)
+StreamFn pick_stream_rk2(bool per, int m, bool xl, int lines)
 {
-    if (per) return xl ? pick_stream_m<true, true>(m) : pick_stream_m<true, false>(m);
-    return xl ? pick_stream_m<false, true>(m) : pick_stream_m<false, false>(m);
+    return per ? pick_stream_l<true>(m, xl, lines) : pick_stream_l<false>(m, xl, lines);
 }
 
 KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant)

@@ -68,10 +68,12 @@ KernelFn pick_kernel_rk1(bool per, bool adj, bool contiguous, int m, int variant
 KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant);
 KernelFn pick_kernel_rk3(bool per, bool adj, bool contiguous, int m, int variant);
 using StreamFn = void (*)(const StreamParams);
-StreamFn pick_stream_rk0(bool per, int m, bool xl);
-StreamFn pick_stream_rk1(bool per, int m, bool xl);
-StreamFn pick_stream_rk2(bool per, int m, bool xl);
-StreamFn pick_stream_rk3(bool per, int m, bool xl);
+// streaming kernels: strided lines are built for 8 or 16 lines per tile
+// (`lines`), x lines for any
+StreamFn pick_stream_rk0(bool per, int m, bool xl, int lines);
+StreamFn pick_stream_rk1(bool per, int m, bool xl, int lines);
+StreamFn pick_stream_rk2(bool per, int m, bool xl, int lines);
+StreamFn pick_stream_rk3(bool per, int m, bool xl, int lines);
 
 // no_fast: every segment on the per-row table (for kernels built for a
 // segment length other than the handle's).

@@ -58,7 +58,8 @@ struct KParams {
     double taps[9];        // adjoint: interior transposed taps
     RhsCoef rc;
     // constant-coefficient interior (see Interior in pado_tables.h)
-    unsigned int_mask;     // bit s: segment s takes the register-only path
+    unsigned int_mask;     // bit s: segment s takes the constant-coefficient path
+    unsigned spk_mask;     // bit s: ... and adds its rows' cyclic spike terms (per-row table)
     double kc[8];          // alpha, c1, c2, gamma, d1, d2, delta
     double pu[KMAXM], pv[KMAXM], ps[KMAXM], pt[KMAXM];  // unit responses, rows 0..m-1
     unsigned char sperm[32];  // thread slot -> segment (per-row-table segments first)
@@ -80,8 +81,8 @@ PADO_HD PADO_INLINE long long line_base(const KParams &kp, long long q)
 // that use it.  etab/toff: the per-row table of the segments that read it,
 // staged in shared memory by the persistent kernel (null: read kp.tab).
 struct Smem {
-    double *buf4;        // [S][L][4]  forward summaries, later backward summaries
-    double *buf2;        // [S][L][2]  forward incoming states, later backward ones
+    double *buf4;        // [S][4][L]  forward summaries, later backward summaries
+    double *buf2;        // [S][2][L]  forward incoming states, later backward ones
     double *eb;          // [L][4]     border unknowns E (0..1) and border rhs (2..3)
     double *ctab;        // [S][KCT_NF] border-sum weights
     double *xtab;        // [S][W][8] transfer products
@@ -110,6 +111,11 @@ PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S, int W)
     (void)P;
     return sm;
 }
+
+// Per-segment summaries, segment-major so that the lanes (lines) of a warp
+// touch consecutive doubles: value k of segment s, line l at p[k * L].
+PADO_HD PADO_INLINE double *sum4(const Smem &sm, int L, int s, int l) { return sm.buf4 + (size_t)s * 4 * L + l; }
+PADO_HD PADO_INLINE double *sum2(const Smem &sm, int L, int s, int l) { return sm.buf2 + (size_t)s * 2 * L + l; }
 
 // Where one line's input comes from and its output goes (set per thread by
 // the kernel driver): row r of the input is src[r * ss], of the output
@@ -273,6 +279,7 @@ struct LineKernel {
     static PADO_HD PADO_INLINE bool fast(const KParams &kp, int s) { return (kp.int_mask >> s) & 1u; }
 
     // ---- constant-coefficient interior segment: stencil + forward sweep ----
+    template <bool STAGED>
     static PADO_HD PADO_INLINE void fwd_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s,
                                              const LineIO &io)
     {
@@ -290,17 +297,24 @@ struct LineKernel {
             for (int t = 0; t < M; ++t) R.r[t] = p[(long long)t * gs];
         }
         const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
-        double z1 = 0.0, z2 = 0.0;
+        double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
+        const bool spk = CYC && ((kp.spk_mask >> s) & 1u);
+        const double *tb = seg_table(kp, sm, s, a);
 #pragma unroll
         for (int t = 0; t < M; ++t) {
             double z = HAS_ALPHA ? al * R.r[t] : R.r[t];
             if (ORDER2) z -= c2 * z2;
             z -= c1 * z1;
             R.r[t] = z;
+            if (CYC && spk) {
+                const double *tr = tb + (size_t)t * T_NF;
+                s1 += tld<STAGED>(tr + T_K1) * z;
+                if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
+            }
             z2 = z1;
             z1 = z;
         }
-        summarize_fwd<false>(kp, sm, l, s, z1, z2, 0.0, 0.0);
+        summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, s1, s2);
     }
 
     // forward summary of segment s: end values y = (z1, z2) and, for a cyclic
@@ -309,39 +323,49 @@ struct LineKernel {
     static PADO_HD PADO_INLINE void summarize_fwd(const KParams &kp, const Smem &sm, int l, int s, double z1,
                                                   double z2, double s1, double s2)
     {
-        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
+        const int L = kp.L;
+        double *o = sum4(sm, L, s, l);
         o[0] = z1;
-        o[1] = z2;
+        o[L] = z2;
         if (CYC) {
             const double *g = (STAGED ? sm.ctab : kp.ctab) + (size_t)s * KCT_NF;
             const Dbl2 g1 = tld2<STAGED>(g), g2 = tld2<STAGED>(g + 2);
-            o[2] = s1 + g1.x * z1 + g1.y * z2;
-            o[3] = s2 + g2.x * z1 + g2.y * z2;
+            o[2 * L] = s1 + g1.x * z1 + g1.y * z2;
+            o[3 * L] = s2 + g2.x * z1 + g2.y * z2;
         }
     }
 
     // ---- constant-coefficient interior segment: backward sweep -------------
     // forward values = local + P1*U + P2*V (the incoming state's response)
+    template <bool STAGED>
     static PADO_HD PADO_INLINE void bwd_fast(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
     {
-        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
+        const double *st = sum2(sm, kp.L, s, l);
         const double ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
-        const double P1 = st[0], P2 = st[1];
+        const double P1 = st[0], P2 = st[kp.L];
+        const bool spk = CYC && ((kp.spk_mask >> s) & 1u);
+        const double E1 = CYC ? sm.eb[(size_t)l * 4 + 0] : 0.0, E2 = CYC ? sm.eb[(size_t)l * 4 + 1] : 0.0;
+        const double *tb = seg_table(kp, sm, s, seg_start(kp, s));
         double x1 = 0.0, x2 = 0.0;
 #pragma unroll
         for (int t = M - 1; t >= 0; --t) {
             double z = R.r[t] + P1 * kp.pu[t];
             if (ORDER2) z += P2 * kp.pv[t];
             double x = ga * z;
+            if (CYC && spk) {
+                const double *tr = tb + (size_t)t * T_NF;
+                x -= tld<STAGED>(tr + T_E1) * E1;
+                if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
+            }
             if (ORDER2) x -= d2 * x2;
             x -= d1 * x1;
             R.r[t] = x;
             x2 = x1;
             x1 = x;
         }
-        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
+        double *o = sum4(sm, kp.L, s, l);
         o[0] = x1;
-        o[1] = x2;
+        o[kp.L] = x2;
     }
 
     // ---- constant-coefficient interior segment: corrections + output ------
@@ -349,9 +373,9 @@ struct LineKernel {
                                              const LineIO &io)
     {
         const int a = seg_start(kp, s);
-        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
+        const double *st = sum2(sm, kp.L, s, l);
         const double de = kp.kc[6];
-        const double Q1 = st[0], Q2 = st[1];
+        const double Q1 = st[0], Q2 = st[kp.L];
         double *p = io.dst + (long long)a * io.ds;
 #pragma unroll
         for (int t = 0; t < M; ++t) {
@@ -375,7 +399,7 @@ struct LineKernel {
         const double *gline = io.src;
         const long long gs = io.ss;
         if (fast(kp, s)) {
-            fwd_fast(kp, sm, R, l, s, io);
+            fwd_fast<STAGED>(kp, sm, R, l, s, io);
             return;
         }
         if (!ADJ) {
@@ -479,27 +503,39 @@ struct LineKernel {
     static PADO_HD PADO_INLINE void chain_fwd(const KParams &kp, const Smem &sm, int l, int s)
     {
         const int L = kp.L, W = kp.W, wf = kp.wf[s];
-        double P1 = 0.0, P2 = 0.0;
+        // four independent partial sums so that the loads of four segments
+        // are in flight together
+        double P1[4] = {0.0, 0.0, 0.0, 0.0}, P2[4] = {0.0, 0.0, 0.0, 0.0};
         const double *xt = sm.xtab + (size_t)s * W * 8;
-        for (int d = 1; d <= wf; ++d) {
-            {
-                const double *y = sm.buf4 + ((size_t)(s - d) * L + l) * 4;
-                const double *ph = xt + (size_t)(d - 1) * 8;
-                const double y0 = y[0], y1 = y[1];
-                P1 += ph[0] * y0 + ph[1] * y1;
-                P2 += ph[2] * y0 + ph[3] * y1;
+        for (int d0 = 1; d0 <= wf; d0 += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int d = d0 + u;
+                if (d <= wf) {
+                    const double *y = sum4(sm, L, s - d, l);
+                    const double *ph = xt + (size_t)(d - 1) * 8;
+                    const double y0 = y[0], y1 = y[L];
+                    P1[u] += ph[0] * y0 + ph[1] * y1;
+                    P2[u] += ph[2] * y0 + ph[3] * y1;
+                }
             }
         }
-        double *st = sm.buf2 + ((size_t)s * L + l) * 2;
-        st[0] = P1;
-        st[1] = P2;
+        double *st = sum2(sm, L, s, l);
+        st[0] = (P1[0] + P1[1]) + (P1[2] + P1[3]);
+        st[L] = (P2[0] + P2[1]) + (P2[2] + P2[3]);
         if (CYC && s == 0) {
-            double sg1 = 0.0, sg2 = 0.0;
-            for (int j = 0; j < kp.S; ++j) {
-                const double *c = sm.buf4 + ((size_t)j * L + l) * 4;
-                sg1 += c[2];
-                sg2 += c[3];
+            double g1[4] = {0.0, 0.0, 0.0, 0.0}, g2[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int j0 = 0; j0 < kp.S; j0 += 4) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (j0 + u < kp.S) {
+                        const double *c = sum4(sm, L, j0 + u, l);
+                        g1[u] += c[2 * L];
+                        g2[u] += c[3 * L];
+                    }
+                }
             }
+            const double sg1 = (g1[0] + g1[1]) + (g1[2] + g1[3]), sg2 = (g2[0] + g2[1]) + (g2[2] + g2[3]);
             double *eb = sm.eb + (size_t)l * 4;
             const double u0 = eb[2] - sg1, u1 = eb[3] - sg2;
             if (kp.nbord == 1) {
@@ -517,14 +553,14 @@ struct LineKernel {
     static PADO_HD PADO_INLINE void bwd(const KParams &kp, const Smem &sm, Regs<M> &R, int l, int s)
     {
         if (fast(kp, s)) {
-            bwd_fast(kp, sm, R, l, s);
+            bwd_fast<STAGED>(kp, sm, R, l, s);
             return;
         }
         const int nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;
-        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-        const double P1 = st[0], P2 = st[1];
+        const double *st = sum2(sm, kp.L, s, l);
+        const double P1 = st[0], P2 = st[kp.L];
         double E1 = 0.0, E2 = 0.0;
         if (CYC) {
             E1 = sm.eb[(size_t)l * 4 + 0];
@@ -566,29 +602,33 @@ struct LineKernel {
                 }
             }
         }
-        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
-        o[0] = x1;  // x at the segment's first row
-        o[1] = x2;  // and the second
+        double *o = sum4(sm, kp.L, s, l);
+        o[0] = x1;     // x at the segment's first row
+        o[kp.L] = x2;  // and the second
     }
 
     // ---- phase chainB: backward incoming states ---------------------------
     static PADO_HD PADO_INLINE void chain_bwd(const KParams &kp, const Smem &sm, int l, int s)
     {
         const int L = kp.L, W = kp.W, wb = kp.wb[s];
-        double Q1 = 0.0, Q2 = 0.0;
+        double Q1[4] = {0.0, 0.0, 0.0, 0.0}, Q2[4] = {0.0, 0.0, 0.0, 0.0};
         const double *xt = sm.xtab + (size_t)s * W * 8 + 4;
-        for (int d = 1; d <= wb; ++d) {
-            {
-                const double *w = sm.buf4 + ((size_t)(s + d) * L + l) * 4;
-                const double *ps_ = xt + (size_t)(d - 1) * 8;
-                const double w0 = w[0], w1 = w[1];
-                Q1 += ps_[0] * w0 + ps_[1] * w1;
-                Q2 += ps_[2] * w0 + ps_[3] * w1;
+        for (int d0 = 1; d0 <= wb; d0 += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int d = d0 + u;
+                if (d <= wb) {
+                    const double *w = sum4(sm, L, s + d, l);
+                    const double *ps_ = xt + (size_t)(d - 1) * 8;
+                    const double w0 = w[0], w1 = w[L];
+                    Q1[u] += ps_[0] * w0 + ps_[1] * w1;
+                    Q2[u] += ps_[2] * w0 + ps_[3] * w1;
+                }
             }
         }
-        double *st = sm.buf2 + ((size_t)s * L + l) * 2;
-        st[0] = Q1;
-        st[1] = Q2;
+        double *st = sum2(sm, L, s, l);
+        st[0] = (Q1[0] + Q1[1]) + (Q1[2] + Q1[3]);
+        st[L] = (Q2[0] + Q2[1]) + (Q2[2] + Q2[3]);
     }
 
     // ---- phase fin: corrected values -> the line's output -----------------
@@ -598,8 +638,8 @@ struct LineKernel {
         const int nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;
-        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-        const double Q1 = st[0], Q2 = st[1];
+        const double *st = sum2(sm, kp.L, s, l);
+        const double Q1 = st[0], Q2 = st[kp.L];
         if (!io.live) return;
         double *line = io.dst;
         const long long gs = io.ds;

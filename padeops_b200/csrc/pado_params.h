@@ -29,6 +29,7 @@ inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn
     kp.rc = ot.rc;
     const Interior &in = ot.interior;
     kp.int_mask = in.mask;
+    kp.spk_mask = in.spk_mask;
     std::memcpy(kp.kc, in.kc, sizeof(kp.kc));
     std::memcpy(kp.pu, in.pu, sizeof(kp.pu));
     std::memcpy(kp.pv, in.pv, sizeof(kp.pv));

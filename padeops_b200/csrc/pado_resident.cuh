@@ -79,6 +79,64 @@ struct ResidentLine {
         }
     }
 
+    // constant-coefficient segment: stencil + forward sweep (w[0..3] preset)
+    template <bool STAGED, bool SPK>
+    static PADO_HD PADO_INLINE void fwd_fast(const KParams &kp, const Smem &sm, double *p, long long rs, int l, int s,
+                                             int a, double (&w)[9], const Halo &h)
+    {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) w[4 + k] = p[(long long)k * rs];
+        const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
+        const double *tbs = SPK ? seg_table(kp, sm, s, a) : nullptr;
+        double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int t = 0; t < M; ++t) {
+            double z = rhs_interior(RK, PER, kp.rc.c, w);
+            if (HAS_ALPHA) z *= al;
+            if (ORDER2) z -= c2 * z2;
+            z -= c1 * z1;
+            p[(long long)t * rs] = z;
+            if (SPK) {
+                const double *tr = tbs + (size_t)t * T_NF;
+                s1 += tld<STAGED>(tr + T_K1) * z;
+                if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
+            }
+            z2 = z1;
+            z1 = z;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
+            if (t + 5 < M) w[8] = p[(long long)(t + 5) * rs];
+            else if (t + 5 - M < 4) w[8] = h.hn[t + 5 - M];
+        }
+        LK::template summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, s1, s2);
+    }
+
+    // constant-coefficient segment: backward sweep, x written over z
+    template <bool STAGED, bool SPK>
+    static PADO_HD PADO_INLINE void bwd_fast(const KParams &kp, const Smem &sm, double *p, long long rs, int l, int s,
+                                             int a, double P1, double P2, double &x1, double &x2)
+    {
+        const double ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
+        const double E1 = SPK ? sm.eb[(size_t)l * 4 + 0] : 0.0, E2 = SPK ? sm.eb[(size_t)l * 4 + 1] : 0.0;
+        const double *tbs = SPK ? seg_table(kp, sm, s, a) : nullptr;
+#pragma unroll
+        for (int t = M - 1; t >= 0; --t) {
+            double z = p[(long long)t * rs] + P1 * kp.pu[t];
+            if (ORDER2) z += P2 * kp.pv[t];
+            double x = ga * z;
+            if (SPK) {
+                const double *tr = tbs + (size_t)t * T_NF;
+                x -= tld<STAGED>(tr + T_E1) * E1;
+                if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
+            }
+            if (ORDER2) x -= d2 * x2;
+            x -= d1 * x1;
+            p[(long long)t * rs] = x;
+            x2 = x1;
+            x1 = x;
+        }
+    }
+
     // ---- fwd: stencil + local forward sweep, z written over f ---------------
     template <bool STAGED>
     static PADO_HD PADO_INLINE void fwd(const KParams &kp, const Smem &sm, double *line, long long rs, int l, int s,
@@ -93,25 +151,11 @@ struct ResidentLine {
         for (int k = 0; k < 4; ++k) w[k] = h.hp[k];
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
         if (fast(kp, s)) {
-            // len == M, every window row inside the line
-#pragma unroll
-            for (int k = 0; k < 5; ++k) w[4 + k] = p[(long long)k * rs];
-            const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
-#pragma unroll
-            for (int t = 0; t < M; ++t) {
-                double z = rhs_interior(RK, PER, kp.rc.c, w);
-                if (HAS_ALPHA) z *= al;
-                if (ORDER2) z -= c2 * z2;
-                z -= c1 * z1;
-                p[(long long)t * rs] = z;
-                z2 = z1;
-                z1 = z;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
-                if (t + 5 < M) w[8] = p[(long long)(t + 5) * rs];
-                else if (t + 5 - M < 4) w[8] = h.hn[t + 5 - M];
-            }
-            LK::template summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, 0.0, 0.0);
+            // len == M, every window row inside the line; the spike terms of
+            // a cyclic line's first segments are a separate instantiation so
+            // that the common path carries no per-row predicates
+            if (CYC && ((kp.spk_mask >> s) & 1u)) fwd_fast<STAGED, true>(kp, sm, p, rs, l, s, a, w, h);
+            else fwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, w, h);
             return;
         }
 #pragma unroll
@@ -166,22 +210,12 @@ struct ResidentLine {
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;
         double *p = line + (long long)a * rs;
-        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-        const double P1 = st[0], P2 = st[1];
+        const double *st = sum2(sm, kp.L, s, l);
+        const double P1 = st[0], P2 = st[kp.L];
         double x1 = 0.0, x2 = 0.0;
         if (fast(kp, s)) {
-            const double ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
-#pragma unroll
-            for (int t = M - 1; t >= 0; --t) {
-                double z = p[(long long)t * rs] + P1 * kp.pu[t];
-                if (ORDER2) z += P2 * kp.pv[t];
-                double x = ga * z;
-                if (ORDER2) x -= d2 * x2;
-                x -= d1 * x1;
-                p[(long long)t * rs] = x;
-                x2 = x1;
-                x1 = x;
-            }
+            if (CYC && ((kp.spk_mask >> s) & 1u)) bwd_fast<STAGED, true>(kp, sm, p, rs, l, s, a, P1, P2, x1, x2);
+            else bwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, P1, P2, x1, x2);
         } else {
             double E1 = 0.0, E2 = 0.0;
             if (CYC) {
@@ -209,9 +243,9 @@ struct ResidentLine {
                 x1 = x;
             }
         }
-        double *o = sm.buf4 + ((size_t)s * kp.L + l) * 4;
-        o[0] = x1;  // x at the segment's first row
-        o[1] = x2;  // and the second
+        double *o = sum4(sm, kp.L, s, l);
+        o[0] = x1;     // x at the segment's first row
+        o[kp.L] = x2;  // and the second
     }
 
     // ---- fin: corrected x -> out (row r at out[r * os]) ----------------------
@@ -225,8 +259,8 @@ struct ResidentLine {
         const int lenb = (a + len <= nb) ? len : nb - a;
         const double *p = line + (long long)a * rs;
         double *q = out + (long long)a * os;
-        const double *st = sm.buf2 + ((size_t)s * kp.L + l) * 2;
-        const double Q1 = st[0], Q2 = st[1];
+        const double *st = sum2(sm, kp.L, s, l);
+        const double Q1 = st[0], Q2 = st[kp.L];
         if (fast(kp, s)) {
 #pragma unroll
             for (int t = 0; t < M; ++t) {

@@ -209,7 +209,9 @@ __device__ __forceinline__ void stream_issue_load(const StreamParams &sp, double
     }
 }
 
-template <int RK, bool PER, int M, bool XL>
+// LT: lines per tile for strided lines, fixed at compile time so that every
+// row offset in the [row][L] tile is an immediate (x lines: 0, L at run time)
+template <int RK, bool PER, int M, bool XL, int LT>
 __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ StreamParams sp)
 {
     using K = LineKernel<RK, PER, false, M, IN_ROWS>;
@@ -219,7 +221,8 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     // that the compiler keeps every access in the shared address space
     double *base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u) / sizeof(double);
     const KParams &kp = sp.kp;
-    const int L = kp.L, S = kp.S;
+    static_assert(XL || LT > 0, "strided lines need a compile-time tile width");
+    const int L = XL ? kp.L : LT, S = kp.S;
     const StreamLayout lay = stream_layout(L, S, kp.W, sp.stages, sp.tile_doubles, sp.etab_rows);
     Smem sm = carve(base + lay.work, L, kp.P, S, kp.W);
     double *etab = base + lay.etab;
@@ -235,7 +238,8 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     const long long t_first = blockIdx.x;
     const int stages = sp.stages;
     // row r of line l in a stage buffer: [row][L] (y, z) or [L][P] (x)
-    const long long rs = XL ? 1 : L, ls = XL ? kp.P : 1;
+    constexpr long long rs = XL ? 1 : LT;
+    const long long ls = XL ? kp.P : 1;
 
     if (tid == 0) {
         for (int b = 0; b < stages; ++b) mbar_init(&bars[b], 1);

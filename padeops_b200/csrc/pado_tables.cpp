@@ -434,21 +434,13 @@ void interior_range(const Sweep &sw, int *i0, int *i1)
     if (nb < 16) return;
     const int mid = nb / 2;
     const double ref[7] = {sw.alpha[mid], sw.c1[mid], sw.c2[mid], sw.gamma[mid], sw.d1[mid], sw.d2[mid], sw.delta[mid]};
-    double kmax = 0.0, emax = 0.0;
-    for (int i = 0; i < nb; ++i) {
-        kmax = std::max({kmax, std::fabs(sw.k1[i]), std::fabs(sw.k2[i])});
-        emax = std::max({emax, std::fabs(sw.e1[i]), std::fabs(sw.e2[i])});
-    }
     // a row is interior when its coefficients equal the line-centre values to
-    // 1e-14 relative (they settle to a few ulps) and its cyclic spike terms
-    // are below 1e-17 of their largest magnitude (their contribution is far
-    // below one rounding of the sums they enter)
+    // 1e-14 relative (they settle to a few ulps); its cyclic spike terms are
+    // handled per row (row_spiky)
     auto ok = [&](int i) {
         const double v[7] = {sw.alpha[i], sw.c1[i], sw.c2[i], sw.gamma[i], sw.d1[i], sw.d2[i], sw.delta[i]};
         for (int k = 0; k < 7; ++k)
             if (std::fabs(v[k] - ref[k]) > 1e-14 * std::fabs(ref[k])) return false;
-        if (std::fabs(sw.k1[i]) > 1e-17 * kmax || std::fabs(sw.k2[i]) > 1e-17 * kmax) return false;
-        if (std::fabs(sw.e1[i]) > 1e-17 * emax || std::fabs(sw.e2[i]) > 1e-17 * emax) return false;
         return true;
     };
     if (!ok(mid)) return;
@@ -541,9 +533,24 @@ Interior interior_info(const Sweep &sw, const Layout &lay, int m)
         in.pt[t] = w;
         x2 = x1; x1 = x; w2 = w1; w1 = w;
     }
+    // cyclic spike terms below 1e-17 of their largest magnitude contribute far
+    // below one rounding of the sums they enter; rows above that keep them
+    double kmax = 0.0, emax = 0.0;
+    for (int i = 0; i < sw.nb; ++i) {
+        kmax = std::max({kmax, std::fabs(sw.k1[i]), std::fabs(sw.k2[i])});
+        emax = std::max({emax, std::fabs(sw.e1[i]), std::fabs(sw.e2[i])});
+    }
+    auto spiky = [&](int i) {
+        return std::fabs(sw.k1[i]) > 1e-17 * kmax || std::fabs(sw.k2[i]) > 1e-17 * kmax ||
+               std::fabs(sw.e1[i]) > 1e-17 * emax || std::fabs(sw.e2[i]) > 1e-17 * emax;
+    };
     for (int s = 1; s + 1 < lay.S && s < 32; ++s) {
         const int a = lay.start(s), len = lay.len(s);
-        if (len == m && a >= i0 && a + len <= i1 && a >= HALO && a + len + HALO <= sw.n) in.mask |= 1u << s;
+        if (len == m && a >= i0 && a + len <= i1 && a >= HALO && a + len + HALO <= sw.n) {
+            in.mask |= 1u << s;
+            for (int i = a; i < a + len; ++i)
+                if (spiky(i)) in.spk_mask |= 1u << s;
+        }
     }
     return in;
 }
@@ -642,7 +649,7 @@ void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsig
     toff.assign(lay.S, 0);
     int rows = 0;
     for (int s = 0; s < lay.S; ++s) {
-        if ((mask >> s) & 1u) continue;
+        if ((mask >> s) & 1u) continue;  // segments that read no per-row values
         const int a = lay.start(s), b = std::min(a + lay.len(s), nb);
         toff[s] = rows;
         for (int i = a; i < b; ++i, ++rows)
@@ -668,7 +675,7 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     ot.interior = interior_info(sw, ot.lay, m);
     ot.chain = chain_tables(ot.tab, segsum, ot.lay, sw.nb, ot.interior, m);
     ot.chain_exact = chain_tables(ot.tab, segsum, ot.lay, sw.nb, Interior{}, m);
-    edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask, ot.etab, ot.toff);
+    edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask & ~ot.interior.spk_mask, ot.etab, ot.toff);
     // thread slots: segments on the per-row table first, so that a warp's
     // segments take one path
     int k = 0;

@@ -66,6 +66,7 @@ void build_device_table(const Sweep &sw, const Layout &lay, std::vector<double> 
 constexpr int MAXM = 64;  // longest segment a kernel is built for
 struct Interior {
     unsigned mask = 0;       // bit s: segment s takes the constant-coefficient path
+    unsigned spk_mask = 0;   // bit s: ... and adds the cyclic spike terms of its rows
     double kc[8] = {0};      // alpha, c1, c2, gamma, d1, d2, delta, (unused)
     // responses of a length-m segment, rows t = 0..m-1: forward sweep to the
     // unit incoming states z_{-1} (pu) and z_{-2} (pv); backward sweep to
@@ -99,8 +100,9 @@ struct ChainTables {
 ChainTables chain_tables(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay, int nb,
                          const Interior &in, int m);
 
-// Rows of the segments that read the per-row table, packed in segment order;
-// toff[s] = first packed row of segment s (0 for constant-coefficient ones).
+// Rows of the segments that read the per-row table (every segment not in
+// `mask`), packed in segment order; toff[s] = first packed row of segment s
+// (0 for the others).
 void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, std::vector<double> &etab,
                 std::vector<int> &toff);
 

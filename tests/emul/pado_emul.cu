@@ -66,6 +66,7 @@ extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, 
     kp.bt = ot.bt.empty() ? nullptr : ot.bt.data();
     if (!fast) {
         kp.int_mask = 0u;
+        kp.spk_mask = 0u;
         for (int i = 0; i < 32; ++i) kp.sperm[i] = (unsigned char)i;
     }
     const int nthreads = lines * lay.S + extra_threads;
