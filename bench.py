@@ -53,9 +53,9 @@ def measured_peaks() -> tuple[float, str]:
 
 
 def profiled_traffic() -> float | None:
-    """DRAM bytes per launch of the line kernel from the committed ncu summary
-    (profiles/line_kernel_512cube.md, line 'traffic_bytes_per_launch: X')."""
-    p = os.path.join(ROOT, "profiles", "line_kernel_512cube.md")
+    """DRAM bytes per 512^3 launch of the streaming kernel from the committed ncu
+    summary (profiles/stream_kernel_512cube.md, line 'traffic_bytes_per_launch: X')."""
+    p = os.path.join(ROOT, "profiles", "stream_kernel_512cube.md")
     try:
         with open(p) as fh:
             for line in fh:
@@ -85,6 +85,11 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start: wait for its first sample
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 5.0:
+                time.sleep(0.02)
+            self.lines.clear()
         except Exception:
             self.proc = None
         return self
@@ -279,7 +284,7 @@ def run_gpu(args) -> None:
                            "per_operator_gbs": per_op},
                 "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(achieved / peak, 4), "traffic": profiled_traffic(),
-                             "kernel": "pado::line_kernel (all 9 launches, averaged)",
+                             "kernel": "pado::stream_kernel (the 9 launches of a step, averaged)",
                              "peak_source": peak_kind},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches}
         print(json.dumps(line), flush=True)
@@ -291,7 +296,7 @@ def run_gpu(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pado", choices=["pado", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

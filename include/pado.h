@@ -138,6 +138,13 @@ int pado_get_tiling(pado_op_t op, int *m, int *lines);
  * PADO_E_UNSUPPORTED otherwise).  Adjoints always use 1.
  * No counterpart in the reference (a B200 tuning knob). */
 int pado_set_kernel_variant(pado_op_t op, int variant);
+/* Tiling of the streaming kernel: lines per tile (8/16 for y/z lines,
+ * 8/16/32 for x lines) and shared-memory stages (1 or 2); 0 leaves the
+ * choice to the occupancy-based planner (the default).  A fixed choice that
+ * does not fit makes the forward operator fall back to variant 1 (variant 0)
+ * or fail with PADO_E_UNSUPPORTED (variant 4).  No counterpart in the
+ * reference (a B200 tuning knob). */
+int pado_set_stream_tiling(pado_op_t op, int lines, int stages);
 /* Device-side status of the handle's kernels: PADO_OK, or PADO_E_TIMEOUT
  * when a streaming kernel's bounded wait for its copies expired (its CTAs
  * then stop early and the output is incomplete).  Synchronous (reads device

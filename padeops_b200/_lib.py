@@ -55,6 +55,7 @@ SIGNATURES = {
     "pado_set_tiling": (_I, [_P, _I, _I]),
     "pado_set_kernel_variant": (_I, [_P, _I]),
     "pado_device_status": (_I, [_P, _I]),
+    "pado_set_stream_tiling": (_I, [_P, _I, _I]),
     "pado_launch_plan": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, ctypes.POINTER(_I)]),
     "pado_get_tiling": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "pado_batch_create": (_I, [ctypes.POINTER(_P), ctypes.POINTER(BatchItem), _I]),

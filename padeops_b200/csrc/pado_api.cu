@@ -100,6 +100,7 @@ int build_tables(pado_op_s *op)
                 if (rc == PADO_OK) rc = upload_vec(op, h.chain_exact.ctab, &dt.ctab_exact);
                 if (rc == PADO_OK) rc = upload_vec(op, h.chain_exact.xtab, &dt.xtab_exact);
                 if (rc == PADO_OK) rc = upload_vec(op, h.etab, &dt.etab);
+                if (rc == PADO_OK) rc = upload_vec(op, h.ktab, &dt.ktab);
                 if (rc == PADO_OK) rc = upload_vec(op, h.toff, &dt.toff);
                 if (rc == PADO_OK) rc = upload_vec(op, h.bt, &dt.bt);
                 if (rc != PADO_OK) return rc;
@@ -193,29 +194,43 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     const size_t align_bits = reinterpret_cast<size_t>(kp0.in) | reinterpret_cast<size_t>(kp0.out);
     if (align_bits & 15) return false;
     if (xl ? (n % 2 != 0) : (na % 2 != 0 || na > 0x7fffffffLL || nb > 0x7fffffffLL)) return false;
-    const int etab_rows = (int)(dt.host.etab.size() / T_NF);
+    if (kp0.nlines > 0x7fffffffLL) return false;  // tile indices are 32-bit in the kernel
+    const int etab_rows = (int)(dt.host.etab.size() / T_NF), ktab_rows = (int)(dt.host.ktab.size() / KT_NF);
+    // candidates in order of preference (measured on 512^3: 16 lines and one
+    // stage, two CTAs per SM, is fastest for every operator); the first that
+    // fits two CTAs per SM wins, else the one with the most resident warps
     int best_warps = 0, bestL = 0, best_stages = 0, best_ctas = 0;
-    for (int L : {16, 32, 8}) {
+    const int cand[6][2] = {{16, 1}, {32, 1}, {8, 1}, {16, 2}, {32, 2}, {8, 2}};
+    for (const auto &c : cand) {
+        const int L = c[0], stages = c[1];
         if (L * S > 384) continue;  // the kernel is built for 384 threads, two CTAs per SM
         if (!xl && L == 32) continue;  // strided-line kernels exist for 8 and 16 lines per tile
+        if (op->stream_lines && L != op->stream_lines) continue;
+        if (op->stream_stages && stages != op->stream_stages) continue;
         StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L);
         if (!grant_smem(fn)) continue;
-        for (int stages : {2, 1}) {
-            const int tile_doubles = stream_tile_doubles(xl, n, L);
-            const size_t bytes = stream_smem_bytes(L, S, kp0.W, stages, tile_doubles, etab_rows);
-            if (bytes > 227 * 1024) continue;
-            int ctas = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, fn, L * S, bytes) != cudaSuccess) {
-                (void)cudaGetLastError();
-                continue;
-            }
-            const int warps = ctas * ((L * S + 31) / 32);
-            if (ctas > 0 && warps > best_warps) {
-                best_warps = warps;
-                bestL = L;
-                best_stages = stages;
-                best_ctas = ctas;
-            }
+        const int tile_doubles = stream_tile_doubles(xl, n, L);
+        const size_t bytes = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows);
+        if (bytes > 227 * 1024) continue;
+        int ctas = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, fn, L * S, bytes) != cudaSuccess) {
+            (void)cudaGetLastError();
+            continue;
+        }
+        if (ctas < 1) continue;
+        const int warps = ctas * ((L * S + 31) / 32);
+        if (ctas >= 2) {
+            best_warps = warps;
+            bestL = L;
+            best_stages = stages;
+            best_ctas = ctas;
+            break;
+        }
+        if (warps > best_warps) {
+            best_warps = warps;
+            bestL = L;
+            best_stages = stages;
+            best_ctas = ctas;
         }
     }
     if (!best_warps) return false;
@@ -229,7 +244,9 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     sp->stages = stages;
     sp->tile_doubles = tile_doubles;
     sp->etab_rows = etab_rows;
+    sp->ktab_rows = ktab_rows;
     sp->etab = dt.etab;
+    sp->ktab = dt.ktab;
     sp->toff = dt.toff;
     sp->status = op->d_status;
     if (xl) {
@@ -256,7 +273,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
             return false;
     }
     *threads = L * S;
-    *smem = stream_smem_bytes(L, S, kp0.W, stages, tile_doubles, etab_rows);
+    *smem = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows);
     *ctas_per_sm = best_ctas;
     return true;
 }
@@ -360,7 +377,7 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
     const bool contiguous = kp.stride == 1;
     const bool persist = !adjoint && (op->variant == 2 || (op->variant == 3 && !contiguous));
     const size_t tile = (adjoint || contiguous) ? (size_t)kp.L * kp.P : (op->variant == 2 ? (size_t)kp.n * kp.L : 0);
-    const size_t smem = smem_doubles(kp.L, kp.S, kp.W, tile) * sizeof(double);
+    const size_t smem = smem_doubles(kp.L, kp.S, kp.xd, tile) * sizeof(double);
     if (smem > 227 * 1024) return PADO_E_SIZE;
     KernelFn fn = pick_kernel(kp.rc.rk, op->periodic != 0, adjoint, contiguous, op->m, op->variant);
     int per_sm = 1;
@@ -570,6 +587,15 @@ int pado_launch_plan(pado_op_t op, int kind, int axis, const double *f, double *
     info[0] = op->variant == 0 ? 1 : op->variant;
     info[1] = kp.L;
     info[6] = kp.L * kp.S;
+    return PADO_OK;
+}
+
+int pado_set_stream_tiling(pado_op_t op, int lines, int stages)
+{
+    if (!op) return PADO_E_NULL;
+    if ((lines != 0 && lines != 8 && lines != 16 && lines != 32) || stages < 0 || stages > 2) return PADO_E_ARG;
+    op->stream_lines = lines;
+    op->stream_stages = stages;
     return PADO_OK;
 }
 

@@ -58,7 +58,7 @@ int layout_items(pado_batch_s *b)
         }
         const int S = kp.S;
         int L = b->threads / std::max(S, 1);
-        while (L > 1 && smem_doubles(L, S, kp.W, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) --L;
+        while (L > 1 && smem_doubles(L, S, kp.xd, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) --L;
         if (L < 1) return PADO_E_SIZE;
         kp.L = L;
         Pre p{};
@@ -67,7 +67,7 @@ int layout_items(pado_batch_s *b)
         const long long tiles = (kp.nlines + L - 1) / L;
         p.d.tile0 = tiles;  // temporarily the tile count
         p.cost = (double)L * kp.n;
-        smem = std::max(smem, smem_doubles(L, kp.S, kp.W, kp.stride == 1 ? (size_t)L * P : 0) * sizeof(double));
+        smem = std::max(smem, smem_doubles(L, kp.S, kp.xd, kp.stride == 1 ? (size_t)L * P : 0) * sizeof(double));
         pre.push_back(p);
     }
     std::stable_sort(pre.begin(), pre.end(), [](const Pre &x, const Pre &y) { return x.cost > y.cost; });

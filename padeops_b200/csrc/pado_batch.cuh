@@ -23,7 +23,7 @@ struct BatchItemDev {
 template <int RK, bool PER, bool STRIDED>
 __device__ __forceinline__ void batch_tile(const KParams &kp, double *smem, long long q0)
 {
-    const Smem sm = carve(smem, kp.L, kp.P, kp.S, kp.W);
+    const Smem sm = carve(smem, kp.L, kp.P, kp.S, kp.xd);
     run_tile<RK, PER, false, BATCH_M, STRIDED ? IN_GLOBAL : IN_LINES>(kp, sm, q0);
 }
 

@@ -9,6 +9,7 @@
 // reference's term grouping; X, Y and Z variants share one formula per row.
 #pragma once
 
+#include <cmath>
 #include <cstddef>
 
 #ifdef __CUDACC__
@@ -174,6 +175,28 @@ PADO_HD PADO_INLINE double rhs_interior(int rk, int periodic, const double *cc, 
     }
 #undef c
 #undef v
+}
+
+// The same interior stencils with fused multiply-adds: for the interior
+// (differences of neighbouring values, no one-sided cancellation) the result
+// moves by a few ulps of the terms, far inside the parity bar, for two to
+// four fewer FP64 operations per row.
+PADO_HD PADO_INLINE double rhs_interior_fma(int rk, int periodic, const double *c, const double *v)
+{
+    switch (rk) {
+    case RHS_CD06_D1:
+        if (periodic) return fma(c[1], v[6] - v[2], c[0] * (v[5] - v[3]));
+        return fma(c[0], v[5] - v[3], c[1] * (v[6] - v[2]));
+    case RHS_CD10_D1:
+        return fma(c[2], v[7] - v[1], fma(c[1], v[6] - v[2], c[0] * (v[5] - v[3])));
+    case RHS_CD10_D2: {
+        const double m2 = -2.0 * v[4];
+        return fma(c[2], v[7] + m2 + v[1], fma(c[1], v[6] + m2 + v[2], c[0] * (v[5] + m2 + v[3])));
+    }
+    default:
+        return fma(c[4], v[8] + v[0],
+                   fma(c[3], v[7] + v[1], fma(c[2], v[6] + v[2], fma(c[1], v[5] + v[3], c[0] * v[4]))));
+    }
 }
 
 // ---------------------------------------------------------------------------

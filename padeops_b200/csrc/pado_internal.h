@@ -29,6 +29,7 @@ struct DevTables {
     double *ctab_exact = nullptr;  // the same with every segment on the per-row table
     double *xtab_exact = nullptr;
     double *etab = nullptr;        // packed rows of the segments that read the table
+    double *ktab = nullptr;        // packed spike values of the spiky interior segments
     int *toff = nullptr;           // [S]
     double *bt = nullptr;          // transposed stencil blocks (adjoint, bounded)
 };
@@ -48,6 +49,7 @@ struct pado_op_s {
     int variant = 0;  // 0: automatic; 1..3: one-CTA-per-tile / persistent kernels; 4: streaming kernel
     int device = 0;
     int *d_status = nullptr;  // device-side status word (bounded waits)
+    int stream_lines = 0, stream_stages = 0;  // streaming kernel tiling (0: chosen by occupancy)
     std::map<pado::TabKey, pado::DevTables> tables;
     std::vector<void *> allocations;
     // host-buffer staging

@@ -51,8 +51,9 @@ struct KParams {
     int bc1, bcn;
     const double *tab;     // [nb][T_NF]
     const double *ctab;    // [S][KCT_NF] border-sum weights G1, G2
-    const double *xtab;    // [S][W][8] transfer products Phi(s, s-d), Psi(s, s+d)
-    int W;                 // segments of coupling kept each way
+    const double *xtab;    // packed transfer products Phi(s, s-d), Psi(s, s+d) (4 doubles each)
+    int W;                 // largest coupling window
+    int xd;                // doubles in xtab
     const double *bt;      // adjoint: transposed stencil blocks (bounded)
     double mb[4];
     double taps[9];        // adjoint: interior transposed taps
@@ -64,7 +65,8 @@ struct KParams {
     double pu[KMAXM], pv[KMAXM], ps[KMAXM], pt[KMAXM];  // unit responses, rows 0..m-1
     unsigned char sperm[32];  // thread slot -> segment (per-row-table segments first)
     unsigned short sstart[33];  // segment s = rows [sstart[s], sstart[s+1])
-    unsigned char wf[32], wb[32];  // coupling window of each segment (forward, backward)
+    unsigned char wf[32], wb[32];    // coupling window of each segment (forward, backward)
+    unsigned short xof[32], xob[32]; // first xtab block of each segment's forward / backward list
 };
 
 // Segment of thread slot `slot` (= tid / L); slots >= S are idle.
@@ -85,19 +87,20 @@ struct Smem {
     double *buf2;        // [S][2][L]  forward incoming states, later backward ones
     double *eb;          // [L][4]     border unknowns E (0..1) and border rhs (2..3)
     double *ctab;        // [S][KCT_NF] border-sum weights
-    double *xtab;        // [S][W][8] transfer products
+    double *xtab;        // packed transfer products (xd doubles)
     double *tile;        // [L][P] or [n][L]
     const double *etab;  // packed table rows of the segments that read the table
     const int *toff;     // [S] first packed row of each segment
+    const double *ktab;  // packed spike values (k1, k2, e1, e2) of the spiky segments' rows
 };
 
 // tile_doubles: 0 (no tile), L*P ([L][P] tile) or n*L ([n][L] tile)
-PADO_HD PADO_INLINE size_t smem_doubles(int L, int S, int W, size_t tile_doubles)
+PADO_HD PADO_INLINE size_t smem_doubles(int L, int S, int xd, size_t tile_doubles)
 {
-    return (size_t)S * L * 6 + (size_t)L * 4 + (size_t)S * KCT_NF + (size_t)S * W * 8 + tile_doubles;
+    return (size_t)S * L * 6 + (size_t)L * 4 + (size_t)S * KCT_NF + (size_t)xd + tile_doubles;
 }
 
-PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S, int W)
+PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S, int xd)
 {
     Smem sm;
     sm.buf4 = base;
@@ -105,9 +108,10 @@ PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S, int W)
     sm.eb = sm.buf2 + (size_t)S * L * 2;
     sm.ctab = sm.eb + (size_t)L * 4;
     sm.xtab = sm.ctab + (size_t)S * KCT_NF;
-    sm.tile = sm.xtab + (size_t)S * W * 8;
+    sm.tile = sm.xtab + (size_t)xd;
     sm.etab = nullptr;
     sm.toff = nullptr;
+    sm.ktab = nullptr;
     (void)P;
     return sm;
 }
@@ -266,6 +270,18 @@ PADO_HD PADO_INLINE Dbl2 tld2(const double *p)
     return ldg2(p);
 }
 
+// Cyclic spike values of the rows of segment s (first row a): the compact
+// staged copy (k1, k2, e1, e2 per row) or the full global table.
+template <bool STAGED>
+struct SpikeRows {
+    static constexpr int STRIDE = STAGED ? 4 : T_NF;
+    static constexpr int K1 = STAGED ? 0 : T_K1, K2 = STAGED ? 1 : T_K2, E1 = STAGED ? 2 : T_E1, E2 = STAGED ? 3 : T_E2;
+    static PADO_HD PADO_INLINE const double *rows(const KParams &kp, const Smem &sm, int s, int a)
+    {
+        return STAGED ? sm.ktab + (size_t)sm.toff[s] * 4 : kp.tab + (size_t)a * T_NF;
+    }
+};
+
 template <int RK, bool PER, bool ADJ, int M, int IN>
 struct LineKernel {
     static constexpr bool CYC = PER;
@@ -299,7 +315,8 @@ struct LineKernel {
         const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
         const bool spk = CYC && ((kp.spk_mask >> s) & 1u);
-        const double *tb = seg_table(kp, sm, s, a);
+        using SR = SpikeRows<STAGED>;
+        const double *tb = SR::rows(kp, sm, s, a);
 #pragma unroll
         for (int t = 0; t < M; ++t) {
             double z = HAS_ALPHA ? al * R.r[t] : R.r[t];
@@ -307,9 +324,9 @@ struct LineKernel {
             z -= c1 * z1;
             R.r[t] = z;
             if (CYC && spk) {
-                const double *tr = tb + (size_t)t * T_NF;
-                s1 += tld<STAGED>(tr + T_K1) * z;
-                if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
+                const double *tr = tb + (size_t)t * SR::STRIDE;
+                s1 += tld<STAGED>(tr + SR::K1) * z;
+                if (ORDER2) s2 += tld<STAGED>(tr + SR::K2) * z;
             }
             z2 = z1;
             z1 = z;
@@ -345,7 +362,8 @@ struct LineKernel {
         const double P1 = st[0], P2 = st[kp.L];
         const bool spk = CYC && ((kp.spk_mask >> s) & 1u);
         const double E1 = CYC ? sm.eb[(size_t)l * 4 + 0] : 0.0, E2 = CYC ? sm.eb[(size_t)l * 4 + 1] : 0.0;
-        const double *tb = seg_table(kp, sm, s, seg_start(kp, s));
+        using SR = SpikeRows<STAGED>;
+        const double *tb = SR::rows(kp, sm, s, seg_start(kp, s));
         double x1 = 0.0, x2 = 0.0;
 #pragma unroll
         for (int t = M - 1; t >= 0; --t) {
@@ -353,9 +371,9 @@ struct LineKernel {
             if (ORDER2) z += P2 * kp.pv[t];
             double x = ga * z;
             if (CYC && spk) {
-                const double *tr = tb + (size_t)t * T_NF;
-                x -= tld<STAGED>(tr + T_E1) * E1;
-                if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
+                const double *tr = tb + (size_t)t * SR::STRIDE;
+                x -= tld<STAGED>(tr + SR::E1) * E1;
+                if (ORDER2) x -= tld<STAGED>(tr + SR::E2) * E2;
             }
             if (ORDER2) x -= d2 * x2;
             x -= d1 * x1;
@@ -502,18 +520,18 @@ struct LineKernel {
     // incoming state is zero, adds up the border sums of its line.
     static PADO_HD PADO_INLINE void chain_fwd(const KParams &kp, const Smem &sm, int l, int s)
     {
-        const int L = kp.L, W = kp.W, wf = kp.wf[s];
+        const int L = kp.L, wf = kp.wf[s];
         // four independent partial sums so that the loads of four segments
         // are in flight together
         double P1[4] = {0.0, 0.0, 0.0, 0.0}, P2[4] = {0.0, 0.0, 0.0, 0.0};
-        const double *xt = sm.xtab + (size_t)s * W * 8;
+        const double *xt = sm.xtab + (size_t)kp.xof[s] * 4;
         for (int d0 = 1; d0 <= wf; d0 += 4) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int d = d0 + u;
                 if (d <= wf) {
                     const double *y = sum4(sm, L, s - d, l);
-                    const double *ph = xt + (size_t)(d - 1) * 8;
+                    const double *ph = xt + (size_t)(d - 1) * 4;
                     const double y0 = y[0], y1 = y[L];
                     P1[u] += ph[0] * y0 + ph[1] * y1;
                     P2[u] += ph[2] * y0 + ph[3] * y1;
@@ -610,16 +628,16 @@ struct LineKernel {
     // ---- phase chainB: backward incoming states ---------------------------
     static PADO_HD PADO_INLINE void chain_bwd(const KParams &kp, const Smem &sm, int l, int s)
     {
-        const int L = kp.L, W = kp.W, wb = kp.wb[s];
+        const int L = kp.L, wb = kp.wb[s];
         double Q1[4] = {0.0, 0.0, 0.0, 0.0}, Q2[4] = {0.0, 0.0, 0.0, 0.0};
-        const double *xt = sm.xtab + (size_t)s * W * 8 + 4;
+        const double *xt = sm.xtab + (size_t)kp.xob[s] * 4;
         for (int d0 = 1; d0 <= wb; d0 += 4) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int d = d0 + u;
                 if (d <= wb) {
                     const double *w = sum4(sm, L, s + d, l);
-                    const double *ps_ = xt + (size_t)(d - 1) * 8;
+                    const double *ps_ = xt + (size_t)(d - 1) * 4;
                     const double w0 = w[0], w1 = w[L];
                     Q1[u] += ps_[0] * w0 + ps_[1] * w1;
                     Q2[u] += ps_[2] * w0 + ps_[3] * w1;
@@ -744,7 +762,7 @@ PADO_HD PADO_INLINE LineIO tile_line_io(const KParams &kp, const Smem &sm, int l
 PADO_HD PADO_INLINE void stage_chain_table(const KParams &kp, const Smem &sm, int tid, int nthreads)
 {
     for (int i = tid; i < kp.S * KCT_NF; i += nthreads) sm.ctab[i] = kp.ctab[i];
-    for (int i = tid; i < kp.S * kp.W * 8; i += nthreads) sm.xtab[i] = kp.xtab[i];
+    for (int i = tid; i < kp.xd; i += nthreads) sm.xtab[i] = kp.xtab[i];
 }
 
 // One tile of kp.L lines on a CTA of nthreads threads (nthreads >= L*S;
@@ -885,7 +903,7 @@ template <int RK, bool PER, bool ADJ, int M, int IN>
 __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line_kernel(const KParams kp)
 {
     extern __shared__ double smem_raw[];
-    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S, kp.W);
+    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S, kp.xd);
     run_tile<RK, PER, ADJ, M, IN>(kp, sm, (long long)blockIdx.x * kp.L);
 }
 
@@ -898,7 +916,7 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
 {
     extern __shared__ double smem_raw[];
     using K = LineKernel<RK, PER, false, M, IN>;
-    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S, kp.W);
+    const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S, kp.xd);
     const int tid = threadIdx.x, nthreads = blockDim.x;
     const int l = tid % kp.L, slot = tid / kp.L, s = slot_segment(kp, slot);
     const bool active = slot < kp.S;
@@ -936,7 +954,7 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
 template <int RK, bool PER, bool ADJ, int M, int IN>
 inline void emulate_tile(const KParams &kp, double *smem, long long q0, int nthreads)
 {
-    const Smem sm = carve(smem, kp.L, kp.P, kp.S, kp.W);
+    const Smem sm = carve(smem, kp.L, kp.P, kp.S, kp.xd);
     Regs<M> *R = new Regs<M>[nthreads];
     if (IN == IN_ROWS)
         for (int tid = 0; tid < nthreads; ++tid) tile_prefetch<IN_ROWS>(kp, sm, q0, tid, nthreads);

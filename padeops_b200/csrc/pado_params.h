@@ -44,8 +44,11 @@ inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn
 inline void set_chain(KParams &kp, const ChainTables &ch)
 {
     kp.W = ch.W;
+    kp.xd = (int)ch.xtab.size();
     std::memcpy(kp.wf, ch.wf, sizeof(kp.wf));
     std::memcpy(kp.wb, ch.wb, sizeof(kp.wb));
+    std::memcpy(kp.xof, ch.xof, sizeof(kp.xof));
+    std::memcpy(kp.xob, ch.xob, sizeof(kp.xob));
 }
 
 // Field geometry of the line family along `axis` of an (n1, n2, n3) field

@@ -87,19 +87,23 @@ struct ResidentLine {
 #pragma unroll
         for (int k = 0; k < 5; ++k) w[4 + k] = p[(long long)k * rs];
         const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
-        const double *tbs = SPK ? seg_table(kp, sm, s, a) : nullptr;
+        double cst[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) cst[k] = kp.rc.c[k];
+        using SR = SpikeRows<STAGED>;
+        const double *tbs = SPK ? SR::rows(kp, sm, s, a) : nullptr;
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
 #pragma unroll
         for (int t = 0; t < M; ++t) {
-            double z = rhs_interior(RK, PER, kp.rc.c, w);
+            double z = rhs_interior_fma(RK, PER, cst, w);
             if (HAS_ALPHA) z *= al;
             if (ORDER2) z -= c2 * z2;
             z -= c1 * z1;
             p[(long long)t * rs] = z;
             if (SPK) {
-                const double *tr = tbs + (size_t)t * T_NF;
-                s1 += tld<STAGED>(tr + T_K1) * z;
-                if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
+                const double *tr = tbs + (size_t)t * SR::STRIDE;
+                s1 += tld<STAGED>(tr + SR::K1) * z;
+                if (ORDER2) s2 += tld<STAGED>(tr + SR::K2) * z;
             }
             z2 = z1;
             z1 = z;
@@ -118,16 +122,17 @@ struct ResidentLine {
     {
         const double ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
         const double E1 = SPK ? sm.eb[(size_t)l * 4 + 0] : 0.0, E2 = SPK ? sm.eb[(size_t)l * 4 + 1] : 0.0;
-        const double *tbs = SPK ? seg_table(kp, sm, s, a) : nullptr;
+        using SR = SpikeRows<STAGED>;
+        const double *tbs = SPK ? SR::rows(kp, sm, s, a) : nullptr;
 #pragma unroll
         for (int t = M - 1; t >= 0; --t) {
             double z = p[(long long)t * rs] + P1 * kp.pu[t];
             if (ORDER2) z += P2 * kp.pv[t];
             double x = ga * z;
             if (SPK) {
-                const double *tr = tbs + (size_t)t * T_NF;
-                x -= tld<STAGED>(tr + T_E1) * E1;
-                if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
+                const double *tr = tbs + (size_t)t * SR::STRIDE;
+                x -= tld<STAGED>(tr + SR::E1) * E1;
+                if (ORDER2) x -= tld<STAGED>(tr + SR::E2) * E2;
             }
             if (ORDER2) x -= d2 * x2;
             x -= d1 * x1;
@@ -163,11 +168,14 @@ struct ResidentLine {
         const double *tb = seg_table(kp, sm, s, a);
         const bool first = !PER && s == 0, last = !PER && s == kp.S - 1;
         double rb0 = 0.0, rb1 = 0.0;
-        // per-row table path: a plain loop (few threads take it; unrolling
-        // it would only add cold code next to the interior path)
-#pragma unroll 1
+        // per-row table path, eight rows per iteration: the window shift is
+        // then register renaming inside the body
+        double cst[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) cst[k] = kp.rc.c[k];
+#pragma unroll 8
         for (int t = 0; t < len; ++t) {
-            double r = rhs_interior(RK, PER, kp.rc.c, w);
+            double r = rhs_interior(RK, PER, cst, w);
             if (first && t < CR) r = pick4(h.cv, t);
             if (last && a + t >= n - CR) r = pick4(h.cl, a + t - (n - CR));
             if (t < lenb) {

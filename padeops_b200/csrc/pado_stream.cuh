@@ -46,50 +46,57 @@ struct alignas(64) StreamParams {
     int box_rows, nbox; // strided lines: rows per tensor copy, copies per tile
     int tile_doubles;   // per stage (a multiple of 16)
     int etab_rows;      // packed table rows staged in shared memory
+    int ktab_rows;      // packed spike rows staged in shared memory
     const double *etab; // [etab_rows][T_NF]
+    const double *ktab; // [ktab_rows][4]
     const int *toff;    // [S]
     int *status;        // PADO_E_TIMEOUT on a wait that expired
 };
 
 // Shared-memory layout, offsets in doubles from a 1024-byte aligned base.
 struct StreamLayout {
-    size_t tiles, work, etab, toff, bars, total_doubles;
+    size_t tiles, work, etab, ktab, toff, bars, total_doubles;
 };
 
-PADO_HD PADO_INLINE StreamLayout stream_layout(int L, int S, int W, int stages, int tile_doubles, int etab_rows)
+PADO_HD PADO_INLINE StreamLayout stream_layout(int L, int S, int xd, int stages, int tile_doubles, int etab_rows,
+                                               int ktab_rows)
 {
     StreamLayout o;
     o.tiles = 0;
     o.work = (size_t)stages * tile_doubles;
-    o.etab = o.work + smem_doubles(L, S, W, 0);
-    o.toff = o.etab + (size_t)etab_rows * T_NF;
+    o.etab = o.work + smem_doubles(L, S, xd, 0);
+    o.ktab = o.etab + (size_t)etab_rows * T_NF;
+    o.toff = o.ktab + (size_t)ktab_rows * 4;
     o.bars = o.toff + (size_t)(S + 1) / 2;
     o.total_doubles = o.bars + (size_t)stages;
     return o;
 }
 
-PADO_HD PADO_INLINE size_t stream_smem_bytes(int L, int S, int W, int stages, int tile_doubles, int etab_rows)
+PADO_HD PADO_INLINE size_t stream_smem_bytes(int L, int S, int xd, int stages, int tile_doubles, int etab_rows,
+                                             int ktab_rows)
 {
-    return stream_layout(L, S, W, stages, tile_doubles, etab_rows).total_doubles * sizeof(double) + 1024;
+    return stream_layout(L, S, xd, stages, tile_doubles, etab_rows, ktab_rows).total_doubles * sizeof(double) + 1024;
 }
 
 // Line l of strided tile t: plane p, lines x0 .. x0+L-1 of that plane.
+// Tile counts fit in 32 bits (the planner checks), and a 32-bit division is
+// a few instructions where a 64-bit one is a long software routine.
 PADO_HD PADO_INLINE void stream_tile_origin(const StreamParams &sp, long long t, long long *x0, long long *p)
 {
     if (sp.axis == 1) {
         *x0 = t * sp.kp.L;
         *p = 0;
     } else {
-        *x0 = (t % sp.xblocks) * sp.kp.L;
-        *p = t / sp.xblocks;
+        const unsigned tu = (unsigned)t, xb = (unsigned)sp.xblocks;
+        const unsigned pq = tu / xb;
+        *x0 = (long long)(tu - pq * xb) * sp.kp.L;
+        *p = pq;
     }
 }
 
-PADO_HD PADO_INLINE LineIO stream_line_io(const StreamParams &sp, const Smem &sm, int l, long long t)
+PADO_HD PADO_INLINE LineIO stream_line_io_at(const StreamParams &sp, const Smem &sm, int l, long long x0, long long p)
 {
     const KParams &kp = sp.kp;
-    long long x0, p;
-    stream_tile_origin(sp, t, &x0, &p);
     LineIO io;
     if (sp.axis == 1) {
         io.live = x0 + l < kp.nlines;
@@ -106,6 +113,14 @@ PADO_HD PADO_INLINE LineIO stream_line_io(const StreamParams &sp, const Smem &sm
         io.ds = kp.stride;
     }
     return io;
+}
+
+PADO_HD PADO_INLINE LineIO stream_line_io(const StreamParams &sp, const Smem &sm, int l, long long t)
+{
+    const KParams &kp = sp.kp;
+    long long x0, p;
+    stream_tile_origin(sp, t, &x0, &p);
+    return stream_line_io_at(sp, sm, l, x0, p);
 }
 
 PADO_HD PADO_INLINE int stream_tile_lines(const StreamParams &sp, long long t)
@@ -129,13 +144,15 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
+// try_wait with a suspend-time hint: the thread sleeps in hardware until the
+// phase completes or about 1 ms passes, instead of spinning on the barrier
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
 {
     unsigned ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(1000000u)
         : "memory");
     return ok != 0;
 }
@@ -223,13 +240,15 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     const KParams &kp = sp.kp;
     static_assert(XL || LT > 0, "strided lines need a compile-time tile width");
     const int L = XL ? kp.L : LT, S = kp.S;
-    const StreamLayout lay = stream_layout(L, S, kp.W, sp.stages, sp.tile_doubles, sp.etab_rows);
-    Smem sm = carve(base + lay.work, L, kp.P, S, kp.W);
+    const StreamLayout lay = stream_layout(L, S, kp.xd, sp.stages, sp.tile_doubles, sp.etab_rows, sp.ktab_rows);
+    Smem sm = carve(base + lay.work, L, kp.P, S, kp.xd);
     double *etab = base + lay.etab;
+    double *ktab = base + lay.ktab;
     int *toff = reinterpret_cast<int *>(base + lay.toff);
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + lay.bars);
     sm.etab = etab;
     sm.toff = toff;
+    sm.ktab = ktab;
 
     const int tid = threadIdx.x, nthreads = blockDim.x;
     const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
@@ -247,6 +266,7 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     }
     stage_chain_table(kp, sm, tid, nthreads);
     for (int i = tid; i < sp.etab_rows * T_NF; i += nthreads) etab[i] = __ldg(sp.etab + i);
+    for (int i = tid; i < sp.ktab_rows * 4; i += nthreads) ktab[i] = __ldg(sp.ktab + i);
     for (int i = tid; i < S; i += nthreads) toff[i] = __ldg(sp.toff + i);
     __syncthreads();
     if (tid == 0) {
@@ -260,7 +280,11 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     for (long long t = t_first; t < sp.ntiles; t += G, ++k) {
         const int b = (int)(k % stages);
         const unsigned parity = (unsigned)((k / stages) & 1);
-        const bool ok = __syncthreads_and(mbar_wait(&bars[b], parity, STREAM_WAIT_NS));
+        // warp 0 polls the barrier; the other warps sleep in the CTA barrier
+        // (spinning warps would take issue slots from the other CTAs on the SM)
+        bool arrived = true;
+        if (tid < 32) arrived = mbar_wait(&bars[b], parity, STREAM_WAIT_NS);
+        const bool ok = __syncthreads_and(arrived);
         if (!ok) {
             // record, let the copies in flight land, and leave
             if (tid == 0) {
@@ -276,7 +300,9 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
         }
         sm.tile = base + (size_t)b * sp.tile_doubles;
         double *line = sm.tile + l * ls;
-        const LineIO io = stream_line_io(sp, sm, l, t);
+        long long x0, p0;
+        stream_tile_origin(sp, t, &x0, &p0);
+        const LineIO io = stream_line_io_at(sp, sm, l, x0, p0);
         typename RL::Halo h;
         if (active) RL::prep(kp, line, rs, s, h);
         __syncthreads();
@@ -294,7 +320,8 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
             // each line's results -> global memory, then the buffer takes the next load
             fence_proxy_async();
             __syncthreads();
-            const int nl = stream_tile_lines(sp, t);
+            const long long nl_ = kp.nlines - x0;
+            const int nl = (int)(nl_ < L ? nl_ : L);
             if (tid < nl) {
                 bulk_store(kp.out + (t * L + tid) * (long long)kp.n, sm.tile + (size_t)tid * kp.P, (unsigned)kp.n * 8u);
                 bulk_commit();
@@ -317,11 +344,14 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
     using RL = ResidentLine<RK, PER, M>;
     const KParams &kp = sp.kp;
     const int L = kp.L, S = kp.S;
-    const StreamLayout lay = stream_layout(L, S, kp.W, 1, sp.tile_doubles, sp.etab_rows);
+    const StreamLayout lay = stream_layout(L, S, kp.xd, 1, sp.tile_doubles, sp.etab_rows, sp.ktab_rows);
     std::vector<double> mem(lay.total_doubles, 0.0);
     double *base = mem.data();
-    Smem sm = carve(base + lay.work, L, kp.P, S, kp.W);
+    Smem sm = carve(base + lay.work, L, kp.P, S, kp.xd);
     double *etab = base + lay.etab;
+    double *ktab = base + lay.ktab;
+    for (int i = 0; i < sp.ktab_rows * 4; ++i) ktab[i] = sp.ktab[i];
+    sm.ktab = ktab;
     int *toff = reinterpret_cast<int *>(base + lay.toff);
     stage_chain_table(kp, sm, 0, 1);
     for (int i = 0; i < sp.etab_rows * T_NF; ++i) etab[i] = sp.etab[i];

@@ -611,19 +611,21 @@ ChainTables chain_tables(const std::vector<double> &tab, const std::vector<doubl
         W = std::max({W, wf, wb});
     }
     ct.W = W;
-    ct.xtab.assign((size_t)S * std::max(W, 1) * 8, 0.0);
-    for (int s = 0; s < S; ++s)
-        for (int d = 1; d <= W; ++d) {
-            double *x = &ct.xtab[((size_t)s * W + (d - 1)) * 8];
-            if (s - d >= 0) {
-                const auto &p = phi[(size_t)s * S + (s - d)];
-                if (norm(p) >= XFER_DROP) std::copy(p.begin(), p.end(), x);
-            }
-            if (s + d < S) {
-                const auto &p = psi[(size_t)s * S + (s + d)];
-                if (norm(p) >= XFER_DROP) std::copy(p.begin(), p.end(), x + 4);
-            }
+    ct.xtab.clear();
+    for (int s = 0; s < S; ++s) {
+        ct.xof[s] = (unsigned short)(ct.xtab.size() / 4);
+        for (int d = 1; d <= ct.wf[s]; ++d) {
+            const auto &p = phi[(size_t)s * S + (s - d)];
+            for (int k = 0; k < 4; ++k) ct.xtab.push_back(norm(p) >= XFER_DROP ? p[k] : 0.0);
         }
+    }
+    for (int s = 0; s < S; ++s) {
+        ct.xob[s] = (unsigned short)(ct.xtab.size() / 4);
+        for (int d = 1; d <= ct.wb[s]; ++d) {
+            const auto &p = psi[(size_t)s * S + (s + d)];
+            for (int k = 0; k < 4; ++k) ct.xtab.push_back(norm(p) >= XFER_DROP ? p[k] : 0.0);
+        }
+    }
     // border-sum weights (every term kept)
     ct.ctab.assign((size_t)S * CT_NF, 0.0);
     for (int j = 0; j < S; ++j) {
@@ -642,18 +644,26 @@ ChainTables chain_tables(const std::vector<double> &tab, const std::vector<doubl
     return ct;
 }
 
-void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, std::vector<double> &etab,
-                std::vector<int> &toff)
+void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, unsigned spk,
+                std::vector<double> &etab, std::vector<double> &ktab, std::vector<int> &toff)
 {
     etab.clear();
+    ktab.clear();
     toff.assign(lay.S, 0);
-    int rows = 0;
+    int rows = 0, krows = 0;
     for (int s = 0; s < lay.S; ++s) {
-        if ((mask >> s) & 1u) continue;  // segments that read no per-row values
         const int a = lay.start(s), b = std::min(a + lay.len(s), nb);
-        toff[s] = rows;
-        for (int i = a; i < b; ++i, ++rows)
-            etab.insert(etab.end(), tab.begin() + (size_t)i * T_NF, tab.begin() + (size_t)(i + 1) * T_NF);
+        if (!((mask >> s) & 1u)) {
+            toff[s] = rows;
+            for (int i = a; i < b; ++i, ++rows)
+                etab.insert(etab.end(), tab.begin() + (size_t)i * T_NF, tab.begin() + (size_t)(i + 1) * T_NF);
+        } else if ((spk >> s) & 1u) {
+            toff[s] = krows;
+            for (int i = a; i < b; ++i, ++krows) {
+                const double *r = &tab[(size_t)i * T_NF];
+                ktab.insert(ktab.end(), {r[T_K1], r[T_K2], r[T_E1], r[T_E2]});
+            }
+        }
     }
 }
 
@@ -675,7 +685,7 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     ot.interior = interior_info(sw, ot.lay, m);
     ot.chain = chain_tables(ot.tab, segsum, ot.lay, sw.nb, ot.interior, m);
     ot.chain_exact = chain_tables(ot.tab, segsum, ot.lay, sw.nb, Interior{}, m);
-    edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask & ~ot.interior.spk_mask, ot.etab, ot.toff);
+    edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask, ot.interior.spk_mask, ot.etab, ot.ktab, ot.toff);
     // thread slots: segments on the per-row table first, so that a warp's
     // segments take one path
     int k = 0;

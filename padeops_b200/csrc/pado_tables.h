@@ -85,7 +85,8 @@ Interior interior_info(const Sweep &sw, const Layout &lay, int m);
 // (y_j, w_j: the local end / first values of segment j).  The products decay
 // like the sweep's homogeneous solutions; those below XFER_DROP are dropped,
 // which bounds the window W.
-//   xtab [S][W][8]: Phi(s, s-d) (4, row-major) and Psi(s, s+d) (4), d = 1..W
+//   xtab: packed 2x2 blocks (4 doubles, row-major): Phi(s, s-d) for d =
+//         1..wf[s] from block xof[s], Psi(s, s+d) for d = 1..wb[s] from xob[s]
 //   ctab [S][CT_NF]: G1_s, G2_s with G_s = sum_{t>s} k_t Phi(t, s), k_t the
 //                    (k.U, k.V) sums of segment t: the cyclic border sums are
 //                    sum_s (local sum_s + G_s . y_s)
@@ -94,17 +95,20 @@ constexpr int CT_NF = 4;
 constexpr double XFER_DROP = 1e-20;
 struct ChainTables {
     std::vector<double> ctab, xtab;
-    int W = 0;
-    unsigned char wf[MAX_SEGMENTS] = {0}, wb[MAX_SEGMENTS] = {0};  // per-segment windows (<= W)
+    int W = 0;  // largest window
+    unsigned char wf[MAX_SEGMENTS] = {0}, wb[MAX_SEGMENTS] = {0};  // per-segment windows
+    unsigned short xof[MAX_SEGMENTS] = {0}, xob[MAX_SEGMENTS] = {0};  // first block of each list
 };
 ChainTables chain_tables(const std::vector<double> &tab, const std::vector<double> &segsum, const Layout &lay, int nb,
                          const Interior &in, int m);
 
 // Rows of the segments that read the per-row table (every segment not in
-// `mask`), packed in segment order; toff[s] = first packed row of segment s
-// (0 for the others).
-void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, std::vector<double> &etab,
-                std::vector<int> &toff);
+// `mask`), packed in segment order (etab, T_NF per row), and the cyclic spike
+// values (k1, k2, e1, e2) of the rows of the segments in `spk` (ktab, 4 per
+// row); toff[s] = first packed row of segment s in its table (0 otherwise).
+constexpr int KT_NF = 4;
+void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, unsigned spk,
+                std::vector<double> &etab, std::vector<double> &ktab, std::vector<int> &toff);
 
 // Everything a kernel launch reads for one (scheme, kind, closures,
 // direction) operator, on the host.
@@ -115,7 +119,7 @@ struct OpTables {
     Layout lay;
     RhsCoef rc{};
     Interior interior;
-    std::vector<double> tab, etab, bt;
+    std::vector<double> tab, etab, ktab, bt;
     ChainTables chain;        // coupling of the segments as the kernels run them
     ChainTables chain_exact;  // with every segment on the per-row table
     std::vector<int> toff;

@@ -112,6 +112,10 @@ class _Scheme:
         keys = ("variant", "lines", "stages", "ctas_per_sm", "segments", "window", "threads", "smem")
         return dict(zip(keys, list(info)))
 
+    def set_stream_tiling(self, lines: int = 0, stages: int = 0) -> None:
+        """Lines per tile and shared-memory stages of the streaming kernel (0 = automatic)."""
+        check(L.lib().pado_set_stream_tiling(self.handle, lines, stages), "set_stream_tiling")
+
     def device_status(self, clear: bool = True) -> int:
         """Status recorded by this handle's kernels (0, or PADO_E_TIMEOUT)."""
         rc = int(L.lib().pado_device_status(self.handle, 1 if clear else 0))

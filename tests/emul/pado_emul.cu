@@ -20,7 +20,7 @@ static void run_all(const KParams &kp, int nthreads)
 {
     const bool strided = kp.stride != 1;
     const size_t tile = (ADJ || !strided) ? (size_t)kp.L * kp.P : (size_t)kp.n * kp.L;
-    std::vector<double> smem(smem_doubles(kp.L, kp.S, kp.W, tile), 0.0);
+    std::vector<double> smem(smem_doubles(kp.L, kp.S, kp.xd, tile), 0.0);
     for (long long q0 = 0; q0 < kp.nlines; q0 += kp.L) {
         if (!strided) emulate_tile<RK, PER, ADJ, M, IN_LINES>(kp, smem.data(), q0, nthreads);
         else if (ADJ) emulate_tile<RK, PER, ADJ, M, IN_GLOBAL>(kp, smem.data(), q0, nthreads);
@@ -115,6 +115,8 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
     sp.stages = 1;
     sp.etab_rows = (int)(ot.etab.size() / T_NF);
     sp.etab = ot.etab.data();
+    sp.ktab_rows = (int)(ot.ktab.size() / KT_NF);
+    sp.ktab = ot.ktab.data();
     sp.toff = ot.toff.data();
     if (xl) {
         kp.P = n + 2;
