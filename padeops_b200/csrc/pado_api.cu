@@ -101,6 +101,7 @@ int build_tables(pado_op_s *op)
                 if (rc == PADO_OK) rc = upload_vec(op, h.chain_exact.xtab, &dt.xtab_exact);
                 if (rc == PADO_OK) rc = upload_vec(op, h.etab, &dt.etab);
                 if (rc == PADO_OK) rc = upload_vec(op, h.ktab, &dt.ktab);
+                if (rc == PADO_OK) rc = upload_vec(op, h.rtab, &dt.rtab);
                 if (rc == PADO_OK) rc = upload_vec(op, h.toff, &dt.toff);
                 if (rc == PADO_OK) rc = upload_vec(op, h.bt, &dt.bt);
                 if (rc != PADO_OK) return rc;
@@ -195,7 +196,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     if (align_bits & 15) return false;
     if (xl ? (n % 2 != 0) : (na % 2 != 0 || na > 0x7fffffffLL || nb > 0x7fffffffLL)) return false;
     if (kp0.nlines > 0x7fffffffLL) return false;  // tile indices are 32-bit in the kernel
-    const int etab_rows = (int)(dt.host.etab.size() / T_NF), ktab_rows = (int)(dt.host.ktab.size() / KT_NF);
+    const int etab_rows = (int)(dt.host.etab.size() / E_NF), ktab_rows = (int)(dt.host.ktab.size() / KT_NF);
     // candidates in order of preference (measured on 512^3: 16 lines and one
     // stage, two CTAs per SM, is fastest for every operator); the first that
     // fits two CTAs per SM wins, else the one with the most resident warps
@@ -210,7 +211,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
         StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L);
         if (!grant_smem(fn)) continue;
         const int tile_doubles = stream_tile_doubles(xl, n, L);
-        const size_t bytes = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows);
+        const size_t bytes = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows, resp_rows(kp0));
         if (bytes > 227 * 1024) continue;
         int ctas = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, fn, L * S, bytes) != cudaSuccess) {
@@ -247,6 +248,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     sp->ktab_rows = ktab_rows;
     sp->etab = dt.etab;
     sp->ktab = dt.ktab;
+    sp->rtab = dt.rtab;
     sp->toff = dt.toff;
     sp->status = op->d_status;
     if (xl) {
@@ -273,7 +275,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
             return false;
     }
     *threads = L * S;
-    *smem = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows);
+    *smem = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows, resp_rows(kp0));
     *ctas_per_sm = best_ctas;
     return true;
 }

@@ -454,6 +454,13 @@ inline RhsCoef make_rhs_coef(int scheme, int kind, double dx, int periodic)
 //
 // Per banded row the device table holds 16 doubles (128 bytes):
 // ---------------------------------------------------------------------------
+// Staged per-row table of the streaming kernel: the fields its sweeps read,
+// pairs that are loaded together kept adjacent.
+enum EtabField {
+    E_C1 = 0, E_C2 = 1, E_ALPHA = 2, E_K1 = 3, E_K2 = 4, E_D2 = 5, E_U = 6, E_V = 7, E_GAMMA = 8, E_D1 = 9,
+    E_S = 10, E_T = 11, E_NF = 12
+};
+
 enum TabField {
     T_C1 = 0, T_C2 = 1, T_ALPHA = 2, T_K1 = 3, T_K2 = 4, T_PAD = 5, T_U = 6, T_V = 7,
     T_GAMMA = 8, T_D1 = 9, T_D2 = 10, T_E1 = 11, T_E2 = 12, T_DELTA = 13, T_S = 14, T_T = 15,

@@ -30,6 +30,7 @@ struct DevTables {
     double *xtab_exact = nullptr;
     double *etab = nullptr;        // packed rows of the segments that read the table
     double *ktab = nullptr;        // packed spike values of the spiky interior segments
+    double *rtab = nullptr;        // border-unknown responses (cyclic lines)
     int *toff = nullptr;           // [S]
     double *bt = nullptr;          // transposed stencil blocks (adjoint, bounded)
 };

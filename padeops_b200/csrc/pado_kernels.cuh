@@ -67,7 +67,16 @@ struct KParams {
     unsigned short sstart[33];  // segment s = rows [sstart[s], sstart[s+1])
     unsigned char wf[32], wb[32];    // coupling window of each segment (forward, backward)
     unsigned short xof[32], xob[32]; // first xtab block of each segment's forward / backward list
+    const double *rtab;    // cyclic: (R1, R2) per row for rows [0, ie) then [je, nb) (streaming kernel)
+    int ie, je;
 };
+
+// Staged response row of banded row i (i < ie or i >= je).
+PADO_HD PADO_INLINE const double *resp_row(const KParams &kp, const double *rtab, int i)
+{
+    return rtab + (size_t)(i < kp.ie ? i : kp.ie + (i - kp.je)) * 2;
+}
+PADO_HD PADO_INLINE int resp_rows(const KParams &kp) { return kp.ie + (kp.nb - kp.je); }
 
 // Segment of thread slot `slot` (= tid / L); slots >= S are idle.
 PADO_HD PADO_INLINE int slot_segment(const KParams &kp, int slot) { return slot < kp.S ? kp.sperm[slot] : slot; }
@@ -91,7 +100,8 @@ struct Smem {
     double *tile;        // [L][P] or [n][L]
     const double *etab;  // packed table rows of the segments that read the table
     const int *toff;     // [S] first packed row of each segment
-    const double *ktab;  // packed spike values (k1, k2, e1, e2) of the spiky segments' rows
+    const double *ktab;  // packed spike values (k1, k2) of the spiky segments' rows
+    const double *rtab;  // staged (R1, R2) rows (streaming kernel)
 };
 
 // tile_doubles: 0 (no tile), L*P ([L][P] tile) or n*L ([n][L] tile)
@@ -112,6 +122,7 @@ PADO_HD PADO_INLINE Smem carve(double *base, int L, int P, int S, int xd)
     sm.etab = nullptr;
     sm.toff = nullptr;
     sm.ktab = nullptr;
+    sm.rtab = nullptr;
     (void)P;
     return sm;
 }
@@ -250,11 +261,15 @@ inline
 
 enum InputSource { IN_GLOBAL = 0, IN_ROWS = 1, IN_LINES = 2 };
 
-// Table rows of segment s (first row a): the staged copy or global memory.
+// Table rows of segment s (first row a) in global memory (T_NF fields per row).
 PADO_HD PADO_INLINE const double *seg_table(const KParams &kp, const Smem &sm, int s, int a)
 {
-    return sm.etab ? sm.etab + (size_t)sm.toff[s] * T_NF : kp.tab + (size_t)a * T_NF;
+    (void)sm;
+    (void)s;
+    return kp.tab + (size_t)a * T_NF;
 }
+// ... and in the streaming kernel's staged copy (E_NF fields per row).
+PADO_HD PADO_INLINE const double *seg_etab(const Smem &sm, int s) { return sm.etab + (size_t)sm.toff[s] * E_NF; }
 
 // Table loads: read-only cache for global memory, plain loads for shared memory.
 template <bool STAGED>
@@ -274,11 +289,11 @@ PADO_HD PADO_INLINE Dbl2 tld2(const double *p)
 // staged copy (k1, k2, e1, e2 per row) or the full global table.
 template <bool STAGED>
 struct SpikeRows {
-    static constexpr int STRIDE = STAGED ? 4 : T_NF;
-    static constexpr int K1 = STAGED ? 0 : T_K1, K2 = STAGED ? 1 : T_K2, E1 = STAGED ? 2 : T_E1, E2 = STAGED ? 3 : T_E2;
+    static constexpr int STRIDE = STAGED ? 2 : T_NF;
+    static constexpr int K1 = STAGED ? 0 : T_K1, K2 = STAGED ? 1 : T_K2, E1 = T_E1, E2 = T_E2;  // E: global only
     static PADO_HD PADO_INLINE const double *rows(const KParams &kp, const Smem &sm, int s, int a)
     {
-        return STAGED ? sm.ktab + (size_t)sm.toff[s] * 4 : kp.tab + (size_t)a * T_NF;
+        return STAGED ? sm.ktab + (size_t)sm.toff[s] * 2 : kp.tab + (size_t)a * T_NF;
     }
 };
 

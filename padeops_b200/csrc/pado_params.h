@@ -36,6 +36,8 @@ inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn
     std::memcpy(kp.ps, in.ps, sizeof(kp.ps));
     std::memcpy(kp.pt, in.pt, sizeof(kp.pt));
     std::memcpy(kp.sperm, ot.sperm, sizeof(kp.sperm));
+    kp.ie = ot.ie;
+    kp.je = ot.nbord > 0 ? ot.je : ot.nb;
     set_chain(kp, ot.chain);
 }
 

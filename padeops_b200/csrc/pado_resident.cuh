@@ -10,11 +10,15 @@
 //   prep    the 4 rows before and after the segment (the neighbours' rows,
 //           read before anyone overwrites them) and the closure rows of a
 //           bounded line
-//   fwd     stencil + local forward sweep; z overwrites f row by row
-//   chainF  incoming forward states (LineKernel::chain_fwd)
-//   bwd     local backward sweep; x overwrites z
-//   chainB  incoming backward states (LineKernel::chain_bwd)
-//   fin     corrected x -> the output line (global memory, or the tile)
+//   fwd     stencil + local forward sweep; z overwrites f row by row; the
+//           segment's end values (and border-sum share) go to buf4
+//   bwd     incoming forward state from the wf[s] segments before (and, for
+//           the segments that need them, the cyclic border unknowns), then
+//           the local backward sweep; x overwrites z; first values -> buf2
+//   fin     incoming backward state from the wb[s] segments after, corrected
+//           x -> the output line (global memory, or the tile)
+// Three barriers separate prep, fwd, bwd and fin: the chains run inside the
+// phases that use them.
 #pragma once
 
 #include "pado_kernels.cuh"
@@ -118,10 +122,9 @@ struct ResidentLine {
     // constant-coefficient segment: backward sweep, x written over z
     template <bool STAGED, bool SPK>
     static PADO_HD PADO_INLINE void bwd_fast(const KParams &kp, const Smem &sm, double *p, long long rs, int l, int s,
-                                             int a, double P1, double P2, double &x1, double &x2)
+                                             int a, double P1, double P2, double E1, double E2, double &x1, double &x2)
     {
         const double ga = kp.kc[3], d1 = kp.kc[4], d2 = kp.kc[5];
-        const double E1 = SPK ? sm.eb[(size_t)l * 4 + 0] : 0.0, E2 = SPK ? sm.eb[(size_t)l * 4 + 1] : 0.0;
         using SR = SpikeRows<STAGED>;
         const double *tbs = SPK ? SR::rows(kp, sm, s, a) : nullptr;
 #pragma unroll
@@ -165,7 +168,7 @@ struct ResidentLine {
         }
 #pragma unroll
         for (int k = 0; k < 5; ++k) w[4 + k] = k < len ? p[(long long)k * rs] : pick4(h.hn, k - len);
-        const double *tb = seg_table(kp, sm, s, a);
+        const double *tb = seg_etab(sm, s);
         const bool first = !PER && s == 0, last = !PER && s == kp.S - 1;
         double rb0 = 0.0, rb1 = 0.0;
         // per-row table path, eight rows per iteration: the window shift is
@@ -179,16 +182,16 @@ struct ResidentLine {
             if (first && t < CR) r = pick4(h.cv, t);
             if (last && a + t >= n - CR) r = pick4(h.cl, a + t - (n - CR));
             if (t < lenb) {
-                const double *tr = tb + (size_t)t * T_NF;
-                const Dbl2 cc = tld2<STAGED>(tr + T_C1);
-                const Dbl2 ak = (HAS_ALPHA || CYC) ? tld2<STAGED>(tr + T_ALPHA) : Dbl2{1.0, 0.0};
+                const double *tr = tb + (size_t)t * E_NF;
+                const Dbl2 cc = tld2<STAGED>(tr + E_C1);
+                const Dbl2 ak = (HAS_ALPHA || CYC) ? tld2<STAGED>(tr + E_ALPHA) : Dbl2{1.0, 0.0};
                 double z = HAS_ALPHA ? ak.x * r : r;
                 if (ORDER2) z -= cc.y * z2;
                 z -= cc.x * z1;
                 p[(long long)t * rs] = z;
                 if (CYC) {
                     s1 += ak.y * z;
-                    if (ORDER2) s2 += tld<STAGED>(tr + T_K2) * z;
+                    if (ORDER2) s2 += tld<STAGED>(tr + E_K2) * z;
                 }
                 z2 = z1;
                 z1 = z;
@@ -210,6 +213,86 @@ struct ResidentLine {
         }
     }
 
+    // ---- incoming states and border unknowns (read the other segments'
+    // summaries; called after the barrier that ends the phase writing them)
+    static PADO_HD PADO_INLINE void incoming_fwd(const KParams &kp, const Smem &sm, int l, int s, double &P1,
+                                                 double &P2)
+    {
+        const int L = kp.L, wf = kp.wf[s];
+        double a1 = 0.0, a2 = 0.0, b1 = 0.0, b2 = 0.0;
+        const double *xt = sm.xtab + (size_t)kp.xof[s] * 4;
+        int d = 1;
+        for (; d + 1 <= wf; d += 2) {
+            const double *y = sum4(sm, L, s - d, l), *yb = sum4(sm, L, s - d - 1, l);
+            const double *ph = xt + (size_t)(d - 1) * 4;
+            const double y0 = y[0], y1 = y[L], z0 = yb[0], z1 = yb[L];
+            a1 += ph[0] * y0 + ph[1] * y1;
+            a2 += ph[2] * y0 + ph[3] * y1;
+            b1 += ph[4] * z0 + ph[5] * z1;
+            b2 += ph[6] * z0 + ph[7] * z1;
+        }
+        if (d <= wf) {
+            const double *y = sum4(sm, L, s - d, l);
+            const double *ph = xt + (size_t)(d - 1) * 4;
+            const double y0 = y[0], y1 = y[L];
+            a1 += ph[0] * y0 + ph[1] * y1;
+            a2 += ph[2] * y0 + ph[3] * y1;
+        }
+        P1 = a1 + b1;
+        P2 = a2 + b2;
+    }
+    static PADO_HD PADO_INLINE void border(const KParams &kp, const Smem &sm, int l, double &E1, double &E2)
+    {
+        const int L = kp.L;
+        double g1[4] = {0.0, 0.0, 0.0, 0.0}, g2[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int j0 = 0; j0 < kp.S; j0 += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (j0 + u < kp.S) {
+                    const double *c = sum4(sm, L, j0 + u, l);
+                    g1[u] += c[2 * L];
+                    g2[u] += c[3 * L];
+                }
+            }
+        }
+        const double sg1 = (g1[0] + g1[1]) + (g1[2] + g1[3]), sg2 = (g2[0] + g2[1]) + (g2[2] + g2[3]);
+        const double *eb = sm.eb + (size_t)l * 4;
+        const double u0 = eb[2] - sg1, u1 = eb[3] - sg2;
+        if (kp.nbord == 1) {
+            E1 = kp.mb[0] * u0;
+            E2 = 0.0;
+        } else {
+            E1 = kp.mb[0] * u0 + kp.mb[1] * u1;
+            E2 = kp.mb[2] * u0 + kp.mb[3] * u1;
+        }
+    }
+    static PADO_HD PADO_INLINE void incoming_bwd(const KParams &kp, const Smem &sm, int l, int s, double &Q1,
+                                                 double &Q2)
+    {
+        const int L = kp.L, wb = kp.wb[s];
+        double a1 = 0.0, a2 = 0.0, b1 = 0.0, b2 = 0.0;
+        const double *xt = sm.xtab + (size_t)kp.xob[s] * 4;
+        int d = 1;
+        for (; d + 1 <= wb; d += 2) {
+            const double *w = sum2(sm, L, s + d, l), *wn = sum2(sm, L, s + d + 1, l);
+            const double *ps_ = xt + (size_t)(d - 1) * 4;
+            const double w0 = w[0], w1 = w[L], v0 = wn[0], v1 = wn[L];
+            a1 += ps_[0] * w0 + ps_[1] * w1;
+            a2 += ps_[2] * w0 + ps_[3] * w1;
+            b1 += ps_[4] * v0 + ps_[5] * v1;
+            b2 += ps_[6] * v0 + ps_[7] * v1;
+        }
+        if (d <= wb) {
+            const double *w = sum2(sm, L, s + d, l);
+            const double *ps_ = xt + (size_t)(d - 1) * 4;
+            const double w0 = w[0], w1 = w[L];
+            a1 += ps_[0] * w0 + ps_[1] * w1;
+            a2 += ps_[2] * w0 + ps_[3] * w1;
+        }
+        Q1 = a1 + b1;
+        Q2 = a2 + b2;
+    }
+
     // ---- bwd: local backward sweep, x written over z ------------------------
     template <bool STAGED>
     static PADO_HD PADO_INLINE void bwd(const KParams &kp, const Smem &sm, double *line, long long rs, int l, int s)
@@ -218,42 +301,58 @@ struct ResidentLine {
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;
         double *p = line + (long long)a * rs;
-        const double *st = sum2(sm, kp.L, s, l);
-        const double P1 = st[0], P2 = st[kp.L];
+        double P1, P2;
+        incoming_fwd(kp, sm, l, s, P1, P2);
         double x1 = 0.0, x2 = 0.0;
+        if (CYC && s == 0) {
+            // the border unknowns, for fin (the sweep itself runs with E = 0)
+            double E1, E2;
+            border(kp, sm, l, E1, E2);
+            sm.eb[(size_t)l * 4 + 0] = E1;
+            sm.eb[(size_t)l * 4 + 1] = E2;
+        }
         if (fast(kp, s)) {
-            if (CYC && ((kp.spk_mask >> s) & 1u)) bwd_fast<STAGED, true>(kp, sm, p, rs, l, s, a, P1, P2, x1, x2);
-            else bwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, P1, P2, x1, x2);
+            bwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, P1, P2, 0.0, 0.0, x1, x2);
         } else {
-            double E1 = 0.0, E2 = 0.0;
-            if (CYC) {
-                E1 = sm.eb[(size_t)l * 4 + 0];
-                E2 = sm.eb[(size_t)l * 4 + 1];
-            }
-            const double *tb = seg_table(kp, sm, s, a);
+            const double *tb = seg_etab(sm, s);
 #pragma unroll 1
             for (int t = lenb - 1; t >= 0; --t) {
-                const double *tr = tb + (size_t)t * T_NF;
-                const Dbl2 uv = tld2<STAGED>(tr + T_U);
-                const Dbl2 gd = tld2<STAGED>(tr + T_GAMMA);
-                const Dbl2 de = tld2<STAGED>(tr + T_D2);
+                const double *tr = tb + (size_t)t * E_NF;
+                const Dbl2 uv = tld2<STAGED>(tr + E_U);
+                const Dbl2 gd = tld2<STAGED>(tr + E_GAMMA);
+                const double d2r = tld<STAGED>(tr + E_D2);
                 double z = p[(long long)t * rs] + P1 * uv.x;
                 if (ORDER2) z += P2 * uv.y;
                 double x = gd.x * z;
-                if (CYC) {
-                    x -= de.y * E1;
-                    if (ORDER2) x -= tld<STAGED>(tr + T_E2) * E2;
-                }
-                if (ORDER2) x -= de.x * x2;
+                if (ORDER2) x -= d2r * x2;
                 x -= gd.y * x1;
                 p[(long long)t * rs] = x;
                 x2 = x1;
                 x1 = x;
             }
         }
-        double *o = sum4(sm, kp.L, s, l);
+        double *o = sum2(sm, kp.L, s, l);
         o[0] = x1;     // x at the segment's first row
         o[kp.L] = x2;  // and the second
+    }
+
+    // constant-coefficient segment: corrected x -> out; RSP: the rows also
+    // take the border unknowns' response E1 R1 + E2 R2
+    template <bool RSP>
+    static PADO_HD PADO_INLINE void fin_fast(const KParams &kp, const Smem &sm, const double *p, long long rs, double *q,
+                                             long long os, int a, double Q1, double Q2, double E1, double E2)
+    {
+#pragma unroll
+        for (int t = 0; t < M; ++t) {
+            double x = p[(long long)t * rs] + Q1 * kp.ps[t];
+            if (ORDER2) x += Q2 * kp.pt[t];
+            if (RSP && (a + t < kp.ie || a + t >= kp.je)) {
+                const double *rr = resp_row(kp, sm.rtab, a + t);
+                x += E1 * rr[0];
+                if (ORDER2) x += E2 * rr[1];
+            }
+            q[(long long)t * os] = x;
+        }
     }
 
     // ---- fin: corrected x -> out (row r at out[r * os]) ----------------------
@@ -267,23 +366,31 @@ struct ResidentLine {
         const int lenb = (a + len <= nb) ? len : nb - a;
         const double *p = line + (long long)a * rs;
         double *q = out + (long long)a * os;
-        const double *st = sum2(sm, kp.L, s, l);
-        const double Q1 = st[0], Q2 = st[kp.L];
+        double Q1, Q2;
+        incoming_bwd(kp, sm, l, s, Q1, Q2);
+        double E1 = 0.0, E2 = 0.0;
+        // rows that take the border unknowns' response
+        const bool spike_rows = CYC && (a < kp.ie || a + len > kp.je);
+        if (spike_rows) {
+            E1 = sm.eb[(size_t)l * 4 + 0];
+            E2 = sm.eb[(size_t)l * 4 + 1];
+        }
         if (fast(kp, s)) {
-#pragma unroll
-            for (int t = 0; t < M; ++t) {
-                double x = p[(long long)t * rs] + Q1 * kp.ps[t];
-                if (ORDER2) x += Q2 * kp.pt[t];
-                q[(long long)t * os] = x;
-            }
+            if (spike_rows) fin_fast<true>(kp, sm, p, rs, q, os, a, Q1, Q2, E1, E2);
+            else fin_fast<false>(kp, sm, p, rs, q, os, a, Q1, Q2, 0.0, 0.0);
             return;
         }
-        const double *tb = seg_table(kp, sm, s, a);
+        const double *tb = seg_etab(sm, s);
 #pragma unroll 2
         for (int t = 0; t < lenb; ++t) {
-            const Dbl2 stt = tld2<STAGED>(tb + (size_t)t * T_NF + T_S);
+            const Dbl2 stt = tld2<STAGED>(tb + (size_t)t * E_NF + E_S);
             double x = p[(long long)t * rs] + Q1 * stt.x;
             if (ORDER2) x += Q2 * stt.y;
+            if (spike_rows && a + t < nb && (a + t < kp.ie || a + t >= kp.je)) {
+                const double *rr = resp_row(kp, sm.rtab, a + t);
+                x += E1 * rr[0];
+                if (ORDER2) x += E2 * rr[1];
+            }
             q[(long long)t * os] = x;
         }
         if (CYC && s == kp.S - 1) {

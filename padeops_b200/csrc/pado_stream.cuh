@@ -8,7 +8,8 @@
 // guarded by an mbarrier.  The sweep runs on the buffer in place
 // (pado_resident.cuh):
 //
-//   wait(full[b])  prep, fwd, chainF, bwd, chainB, fin (barrier-separated)
+//   wait(full[b])  prep, fwd, bwd, fin (barrier-separated; the chains run
+//                  inside bwd and fin)
 //   strided lines: results to global memory from fin
 //   x lines:       fin writes the buffer; bulk store of each line
 //   then the load `stages` tiles ahead is issued into buffer b
@@ -47,35 +48,38 @@ struct alignas(64) StreamParams {
     int tile_doubles;   // per stage (a multiple of 16)
     int etab_rows;      // packed table rows staged in shared memory
     int ktab_rows;      // packed spike rows staged in shared memory
-    const double *etab; // [etab_rows][T_NF]
-    const double *ktab; // [ktab_rows][4]
+    const double *rtab; // [resp_rows][2] border-unknown responses (cyclic lines)
+    const double *etab; // [etab_rows][E_NF]
+    const double *ktab; // [ktab_rows][2]
     const int *toff;    // [S]
     int *status;        // PADO_E_TIMEOUT on a wait that expired
 };
 
 // Shared-memory layout, offsets in doubles from a 1024-byte aligned base.
 struct StreamLayout {
-    size_t tiles, work, etab, ktab, toff, bars, total_doubles;
+    size_t tiles, work, etab, ktab, rtab, toff, bars, total_doubles;
 };
 
 PADO_HD PADO_INLINE StreamLayout stream_layout(int L, int S, int xd, int stages, int tile_doubles, int etab_rows,
-                                               int ktab_rows)
+                                               int ktab_rows, int ie)
 {
     StreamLayout o;
     o.tiles = 0;
     o.work = (size_t)stages * tile_doubles;
     o.etab = o.work + smem_doubles(L, S, xd, 0);
-    o.ktab = o.etab + (size_t)etab_rows * T_NF;
-    o.toff = o.ktab + (size_t)ktab_rows * 4;
+    o.ktab = o.etab + (size_t)etab_rows * E_NF;
+    o.rtab = o.ktab + (size_t)ktab_rows * 2;
+    o.toff = o.rtab + (size_t)ie * 2;
     o.bars = o.toff + (size_t)(S + 1) / 2;
     o.total_doubles = o.bars + (size_t)stages;
     return o;
 }
 
 PADO_HD PADO_INLINE size_t stream_smem_bytes(int L, int S, int xd, int stages, int tile_doubles, int etab_rows,
-                                             int ktab_rows)
+                                             int ktab_rows, int ie)
 {
-    return stream_layout(L, S, xd, stages, tile_doubles, etab_rows, ktab_rows).total_doubles * sizeof(double) + 1024;
+    return stream_layout(L, S, xd, stages, tile_doubles, etab_rows, ktab_rows, ie).total_doubles * sizeof(double) +
+           1024;
 }
 
 // Line l of strided tile t: plane p, lines x0 .. x0+L-1 of that plane.
@@ -240,15 +244,18 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     const KParams &kp = sp.kp;
     static_assert(XL || LT > 0, "strided lines need a compile-time tile width");
     const int L = XL ? kp.L : LT, S = kp.S;
-    const StreamLayout lay = stream_layout(L, S, kp.xd, sp.stages, sp.tile_doubles, sp.etab_rows, sp.ktab_rows);
+    const StreamLayout lay =
+        stream_layout(L, S, kp.xd, sp.stages, sp.tile_doubles, sp.etab_rows, sp.ktab_rows, resp_rows(kp));
     Smem sm = carve(base + lay.work, L, kp.P, S, kp.xd);
     double *etab = base + lay.etab;
     double *ktab = base + lay.ktab;
+    double *rtab = base + lay.rtab;
     int *toff = reinterpret_cast<int *>(base + lay.toff);
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + lay.bars);
     sm.etab = etab;
     sm.toff = toff;
     sm.ktab = ktab;
+    sm.rtab = rtab;
 
     const int tid = threadIdx.x, nthreads = blockDim.x;
     const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
@@ -265,8 +272,9 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
         mbar_fence_init();
     }
     stage_chain_table(kp, sm, tid, nthreads);
-    for (int i = tid; i < sp.etab_rows * T_NF; i += nthreads) etab[i] = __ldg(sp.etab + i);
-    for (int i = tid; i < sp.ktab_rows * 4; i += nthreads) ktab[i] = __ldg(sp.ktab + i);
+    for (int i = tid; i < sp.etab_rows * E_NF; i += nthreads) etab[i] = __ldg(sp.etab + i);
+    for (int i = tid; i < sp.ktab_rows * 2; i += nthreads) ktab[i] = __ldg(sp.ktab + i);
+    for (int i = tid; i < resp_rows(kp) * 2; i += nthreads) rtab[i] = __ldg(sp.rtab + i);
     for (int i = tid; i < S; i += nthreads) toff[i] = __ldg(sp.toff + i);
     __syncthreads();
     if (tid == 0) {
@@ -308,11 +316,7 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
         __syncthreads();
         if (active) RL::template fwd<true>(kp, sm, line, rs, l, s, h);
         __syncthreads();
-        if (active) K::chain_fwd(kp, sm, l, s);
-        __syncthreads();
         if (active) RL::template bwd<true>(kp, sm, line, rs, l, s);
-        __syncthreads();
-        if (active) K::chain_bwd(kp, sm, l, s);
         __syncthreads();
         if (active) RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live);
         const long long tn = t + (long long)stages * G;  // tile for this buffer next
@@ -344,17 +348,21 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
     using RL = ResidentLine<RK, PER, M>;
     const KParams &kp = sp.kp;
     const int L = kp.L, S = kp.S;
-    const StreamLayout lay = stream_layout(L, S, kp.xd, 1, sp.tile_doubles, sp.etab_rows, sp.ktab_rows);
+    const StreamLayout lay =
+        stream_layout(L, S, kp.xd, 1, sp.tile_doubles, sp.etab_rows, sp.ktab_rows, resp_rows(kp));
     std::vector<double> mem(lay.total_doubles, 0.0);
     double *base = mem.data();
     Smem sm = carve(base + lay.work, L, kp.P, S, kp.xd);
     double *etab = base + lay.etab;
     double *ktab = base + lay.ktab;
-    for (int i = 0; i < sp.ktab_rows * 4; ++i) ktab[i] = sp.ktab[i];
+    double *rtab = base + lay.rtab;
+    for (int i = 0; i < sp.ktab_rows * 2; ++i) ktab[i] = sp.ktab[i];
+    for (int i = 0; i < resp_rows(kp) * 2; ++i) rtab[i] = sp.rtab[i];
     sm.ktab = ktab;
+    sm.rtab = rtab;
     int *toff = reinterpret_cast<int *>(base + lay.toff);
     stage_chain_table(kp, sm, 0, 1);
-    for (int i = 0; i < sp.etab_rows * T_NF; ++i) etab[i] = sp.etab[i];
+    for (int i = 0; i < sp.etab_rows * E_NF; ++i) etab[i] = sp.etab[i];
     for (int i = 0; i < S; ++i) toff[i] = sp.toff[i];
     sm.etab = etab;
     sm.toff = toff;
@@ -375,6 +383,7 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
             }
         }
         for (int ph = 0; ph < 6; ++ph) {
+            if (ph == 2 || ph == 4) continue;  // the chains run inside bwd and fin
             for (int tid = 0; tid < nthreads; ++tid) {
                 const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
                 if (slot >= S) continue;

@@ -655,13 +655,28 @@ void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsig
         const int a = lay.start(s), b = std::min(a + lay.len(s), nb);
         if (!((mask >> s) & 1u)) {
             toff[s] = rows;
-            for (int i = a; i < b; ++i, ++rows)
-                etab.insert(etab.end(), tab.begin() + (size_t)i * T_NF, tab.begin() + (size_t)(i + 1) * T_NF);
+            for (int i = a; i < b; ++i, ++rows) {
+                const double *r = &tab[(size_t)i * T_NF];
+                double e[E_NF];
+                e[E_C1] = r[T_C1];
+                e[E_C2] = r[T_C2];
+                e[E_ALPHA] = r[T_ALPHA];
+                e[E_K1] = r[T_K1];
+                e[E_K2] = r[T_K2];
+                e[E_D2] = r[T_D2];
+                e[E_U] = r[T_U];
+                e[E_V] = r[T_V];
+                e[E_GAMMA] = r[T_GAMMA];
+                e[E_D1] = r[T_D1];
+                e[E_S] = r[T_S];
+                e[E_T] = r[T_T];
+                etab.insert(etab.end(), e, e + E_NF);
+            }
         } else if ((spk >> s) & 1u) {
             toff[s] = krows;
             for (int i = a; i < b; ++i, ++krows) {
                 const double *r = &tab[(size_t)i * T_NF];
-                ktab.insert(ktab.end(), {r[T_K1], r[T_K2], r[T_E1], r[T_E2]});
+                ktab.insert(ktab.end(), {r[T_K1], r[T_K2]});
             }
         }
     }
@@ -686,6 +701,36 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     ot.chain = chain_tables(ot.tab, segsum, ot.lay, sw.nb, ot.interior, m);
     ot.chain_exact = chain_tables(ot.tab, segsum, ot.lay, sw.nb, Interior{}, m);
     edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask, ot.interior.spk_mask, ot.etab, ot.ktab, ot.toff);
+    if (sw.nbord > 0) {
+        // backward sweep of the unit spike sources: x_i = -e_i - d1_i x_{i+1} - d2_i x_{i+2}
+        const int nb = sw.nb;
+        std::vector<double> r1(nb + 2, 0.0), r2(nb + 2, 0.0);
+        double rmax = 0.0;
+        for (int i = nb - 1; i >= 0; --i) {
+            r1[i] = -sw.e1[i] - sw.d1[i] * r1[i + 1] - sw.d2[i] * r1[i + 2];
+            r2[i] = -sw.e2[i] - sw.d1[i] * r2[i + 1] - sw.d2[i] * r2[i + 2];
+            rmax = std::max({rmax, std::fabs(r1[i]), std::fabs(r2[i])});
+        }
+        auto big = [&](int i) { return std::fabs(r1[i]) > 1e-17 * rmax || std::fabs(r2[i]) > 1e-17 * rmax; };
+        // the longest run of negligible rows splits the line into the two regions
+        int best_a = nb, best_b = nb, run_a = -1;
+        for (int i = 0; i <= nb; ++i) {
+            const bool small = i < nb && !big(i);
+            if (small && run_a < 0) run_a = i;
+            if (!small && run_a >= 0) {
+                if (i - run_a > best_b - best_a) {
+                    best_a = run_a;
+                    best_b = i;
+                }
+                run_a = -1;
+            }
+        }
+        ot.ie = best_a;
+        ot.je = best_b;
+        ot.rtab.clear();
+        for (int i = 0; i < nb; ++i)
+            if (i < ot.ie || i >= ot.je) ot.rtab.insert(ot.rtab.end(), {r1[i], r2[i]});
+    }
     // thread slots: segments on the per-row table first, so that a warp's
     // segments take one path
     int k = 0;

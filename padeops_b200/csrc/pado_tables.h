@@ -103,10 +103,11 @@ ChainTables chain_tables(const std::vector<double> &tab, const std::vector<doubl
                          const Interior &in, int m);
 
 // Rows of the segments that read the per-row table (every segment not in
-// `mask`), packed in segment order (etab, T_NF per row), and the cyclic spike
-// values (k1, k2, e1, e2) of the rows of the segments in `spk` (ktab, 4 per
-// row); toff[s] = first packed row of segment s in its table (0 otherwise).
-constexpr int KT_NF = 4;
+// `mask`), packed in segment order (etab, the E_NF fields of EtabField per
+// row), and the cyclic sums' spike values (k1, k2) of the rows of the
+// segments in `spk` (ktab, 2 per row); toff[s] = first packed row of segment s
+// in its table (0 otherwise).
+constexpr int KT_NF = 2;
 void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, unsigned spk,
                 std::vector<double> &etab, std::vector<double> &ktab, std::vector<int> &toff);
 
@@ -120,6 +121,12 @@ struct OpTables {
     RhsCoef rc{};
     Interior interior;
     std::vector<double> tab, etab, ktab, bt;
+    // cyclic lines: responses of the backward sweep to its spike columns,
+    // x = x(E = 0) + E1 R1 + E2 R2, kept on rows [0, ie) and [je, nb) (in
+    // between they are below 1e-17 of their largest magnitude), stored as
+    // (R1, R2) pairs, the rows of [0, ie) first
+    std::vector<double> rtab;
+    int ie = 0, je = 0;
     ChainTables chain;        // coupling of the segments as the kernels run them
     ChainTables chain_exact;  // with every segment on the per-row table
     std::vector<int> toff;

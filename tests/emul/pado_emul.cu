@@ -113,10 +113,11 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
     const bool xl = axis == 1;
     sp.axis = axis;
     sp.stages = 1;
-    sp.etab_rows = (int)(ot.etab.size() / T_NF);
+    sp.etab_rows = (int)(ot.etab.size() / E_NF);
     sp.etab = ot.etab.data();
     sp.ktab_rows = (int)(ot.ktab.size() / KT_NF);
     sp.ktab = ot.ktab.data();
+    sp.rtab = ot.rtab.data();
     sp.toff = ot.toff.data();
     if (xl) {
         kp.P = n + 2;
