@@ -234,3 +234,20 @@ def test_launch_count_and_library(torch_cuda):
     op.dd2(f, df, 3, 3)
     torch.cuda.synchronize()
     assert pb.launch_count() == before + 1
+
+
+def test_parity_golden_fixtures(torch_cuda):
+    """The committed fixtures (tests/golden/oracle_small.npz, written by
+    tests/golden/make_golden.py): every operator, both boundary kinds, every
+    closure pair along x (cd06 with its closures fixed at init) and all axes."""
+    import json
+    import os
+
+    torch = torch_cuda
+    data = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_small.npz"))
+    cases = json.loads(str(data["cases"]))
+    for i, c in enumerate(cases):
+        op = _make(c["scheme"], c["n"], c["dx"], c["periodic"], c["ibc1"], c["ibcn"])
+        got = _gpu_apply(torch, op, c["kind"], c["axis"], data[f"f{i}"], c["bc1"], c["bcn"])
+        ref = data[f"df{i}"]
+        assert rel_err(got, ref) <= TOL, (c, rel_err(got, ref))
