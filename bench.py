@@ -293,6 +293,33 @@ def run_gpu(args) -> None:
         dist.destroy_process_group()
 
 
+def run_single_op(args) -> None:
+    """One operator on one field, a few times: the small cases the ncu summaries
+    under profiles/ are captured on (prints the launch plan)."""
+    import torch
+
+    import padeops_b200 as pb
+
+    scheme, kind, axis = args.op.split(":")
+    kind, axis = int(kind), int(axis)
+    n3, n2, n1 = (int(v) for v in args.shape.split(","))
+    n = {1: n1, 2: n2, 3: n3}[axis]
+    na, nb = {1: (n2, n3), 2: (n1, n3), 3: (n1, n2)}[axis]
+    periodic = not args.bounded
+    op = {"cd06": pb.cd06, "cd10": pb.cd10, "cf90": pb.cf90}[scheme]()
+    ierr = op.init(n, periodic) if scheme == "cf90" else op.init(n, 2 * np.pi / n, periodic, 0, 0)
+    assert ierr == 0, ierr
+    g = torch.Generator(device="cuda").manual_seed(7)
+    f = torch.randn(n1 * n2 * n3, dtype=torch.float64, device="cuda", generator=g)
+    df = torch.empty_like(f)
+    print(json.dumps({"op": args.op, "shape": [n3, n2, n1], "periodic": periodic,
+                      "plan": op.launch_plan(kind, axis, f, df, na, nb)}), flush=True)
+    for _ in range(args.repeat):
+        op.apply(kind, axis, f, df, na, nb)
+    torch.cuda.synchronize()
+    assert op.device_status() == 0
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,8 +327,14 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pado", choices=["pado", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--op", default=None, help="profiling: run only scheme:kind:axis (e.g. cf90:0:3)")
+    ap.add_argument("--shape", default="512,128,512", help="profiling: field shape n3,n2,n1")
+    ap.add_argument("--bounded", action="store_true", help="profiling: bounded instead of periodic lines")
+    ap.add_argument("--repeat", type=int, default=3, help="profiling: applications of the operator")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.op:
+        run_single_op(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
