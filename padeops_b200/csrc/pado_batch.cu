@@ -59,7 +59,7 @@ int layout_items(pado_batch_s *b)
         const int S = kp.S;
         int L = b->threads / std::max(S, 1);
         while (L > 1 && smem_doubles(L, S, kp.xd, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) --L;
-        if (L < 1) return PADO_E_SIZE;
+        if (L < 1 || smem_doubles(L, S, kp.xd, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) return PADO_E_SIZE;
         kp.L = L;
         Pre p{};
         p.d.kp = kp;
@@ -98,8 +98,10 @@ int upload_batch(pado_batch_s *b)
         cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
         if (e != cudaSuccess) return cuda_fail(e);
     }
+    // The attribute is per function, shared by every batch: always the cap (every
+    // batch's smem is below it), so creating one batch never invalidates another.
     cudaError_t e = cudaFuncSetAttribute((const void *)batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)std::max<size_t>(b->smem, 1024));
+                                         (int)BATCH_SMEM_CAP);
     if (e != cudaSuccess) return cuda_fail(e);
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, b->threads, b->smem);
