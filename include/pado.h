@@ -186,6 +186,31 @@ int pado_batch_set_config(pado_batch_t batch, int threads, int ctas_per_sm);
 int pado_batch_info(pado_batch_t batch, long long *ntiles, int *grid, int *threads, long long *smem_bytes);
 void pado_batch_destroy(pado_batch_t batch);
 
+/* Most items one pado_batch_run_static call accepts. */
+#define PADO_STATIC_BATCH_MAX_ITEMS 256
+/* Bytes of the library's fixed device scratch array behind pado_batch_run_static. */
+#define PADO_STATIC_BATCH_SCRATCH_BYTES (768 * 1024)
+
+/* The batched launch for callers that may not allocate device memory once
+ * they are running: a solver that hands all of HBM to its own pool at start-up,
+ * or one that builds a different list of fields every time step and may not
+ * pay for (or is not allowed) a cudaMalloc/cudaFree per step.  Does what
+ * pado_batch_create + pado_batch_run + pado_batch_destroy do, but calls no
+ * cudaMalloc or cudaFree: the item descriptors and the tile counter live in
+ * a fixed 768 KiB array inside the library (held on every GPU that loads it
+ * until the process exits).  The operators' own tables are made by their
+ * init, as usual.  The caller passes the inputs and outputs as in
+ * pado_batch_item.
+ *   - nitems above PADO_STATIC_BATCH_MAX_ITEMS returns PADO_E_SIZE.
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current); make it before any stream capture.
+ *   - All calls on a device share the one array: two calls whose launches
+ *     overlap on the GPU race and give wrong results.  Order them on one
+ *     stream, or wait for one before starting the next.
+ *   - Every item's operator must belong to the current device.
+ * No counterpart in the reference. */
+int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream);
+
 /* ---- diagnostics -------------------------------------------------------- */
 
 const char *pado_strerror(int status);

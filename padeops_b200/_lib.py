@@ -17,6 +17,7 @@ FILTER, D1, D2 = 0, 1, 2
 OK = 0
 E_BC = 324
 E_NULL, E_ALIAS, E_UNSUPPORTED, E_ARG, E_CUDA, E_SIZE, E_TIMEOUT, E_NOMEM, E_STATE = -1, -2, -3, -4, -5, -6, -7, -8, -9
+STATIC_BATCH_MAX_ITEMS = 256  # PADO_STATIC_BATCH_MAX_ITEMS
 
 
 class PadoError(RuntimeError):
@@ -66,6 +67,7 @@ SIGNATURES = {
     "pado_batch_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I), ctypes.POINTER(_I),
                              ctypes.POINTER(ctypes.c_longlong)]),
     "pado_batch_destroy": (None, [_P]),
+    "pado_batch_run_static": (_I, [_P, _I, _P]),
     "pado_strerror": (ctypes.c_char_p, [_I]),
     "pado_launch_count": (ctypes.c_longlong, []),
     "pado_version": (ctypes.c_char_p, []),
