@@ -135,7 +135,8 @@ int pado_get_tiling(pado_op_t op, int *m, int *lines);
  * (strided axes; x lines use 2), 4 = the streaming kernel: persistent CTAs
  * fed by TMA tensor / bulk copies two tiles ahead (needs 16-byte aligned
  * fields, an even x extent for y/z lines and an even n for x lines;
- * PADO_E_UNSUPPORTED otherwise).  Adjoints always use 1.
+ * PADO_E_UNSUPPORTED otherwise).  Adjoints follow the same choice (4 runs
+ * the transposed sweep in the tile, then B^T); 2 and 3 mean 1 for adjoints.
  * No counterpart in the reference (a B200 tuning knob). */
 int pado_set_kernel_variant(pado_op_t op, int variant);
 /* Tiling of the streaming kernel: lines per tile (8/16 for y/z lines,

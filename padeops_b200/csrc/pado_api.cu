@@ -44,6 +44,10 @@ bool kind_supported(int scheme, int kind)
 
 namespace {
 
+// host-buffer pipeline: about this many bytes per chunk, at most this many chunks
+constexpr size_t HOST_CHUNK_BYTES = size_t(64) << 20;
+constexpr size_t HOST_MAX_CHUNKS = 32;
+
 int max_threads_for_m(int m) { return m >= 64 ? 256 : 512; }
 
 // Default tiling: segment length and lines per CTA for a line of length n.
@@ -142,13 +146,13 @@ EncodeTiledFn encode_tiled()
     return fn;
 }
 
-StreamFn pick_stream(int rk, bool per, int m, bool xl, int lines)
+StreamFn pick_stream(int rk, bool per, int m, bool xl, int lines, bool adj)
 {
     switch (rk) {
-    case RHS_CD06_D1: return pick_stream_rk0(per, m, xl, lines);
-    case RHS_CD10_D1: return pick_stream_rk1(per, m, xl, lines);
-    case RHS_CD10_D2: return pick_stream_rk2(per, m, xl, lines);
-    default: return pick_stream_rk3(per, m, xl, lines);
+    case RHS_CD06_D1: return pick_stream_rk0(per, m, xl, lines, adj);
+    case RHS_CD10_D1: return pick_stream_rk1(per, m, xl, lines, adj);
+    case RHS_CD10_D2: return pick_stream_rk2(per, m, xl, lines, adj);
+    default: return pick_stream_rk3(per, m, xl, lines, adj);
     }
 }
 
@@ -187,7 +191,7 @@ bool grant_smem(StreamFn fn)
 // a table too large to stage); the caller then runs the one-CTA-per-tile
 // kernel.
 bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, int axis, long long na, long long nb,
-                 StreamParams *sp, int *threads, size_t *smem, int *ctas_per_sm)
+                 bool adj, StreamParams *sp, int *threads, size_t *smem, int *ctas_per_sm)
 {
     const int n = op->n, S = kp0.S;
     if (op->m != 16 && op->m != 32 && op->m != 64) return false;
@@ -208,7 +212,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
         if (!xl && L == 32) continue;  // strided-line kernels exist for 8 and 16 lines per tile
         if (op->stream_lines && L != op->stream_lines) continue;
         if (op->stream_stages && stages != op->stream_stages) continue;
-        StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L);
+        StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L, adj);
         if (!grant_smem(fn)) continue;
         const int tile_doubles = stream_tile_doubles(xl, n, L);
         const size_t bytes = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows, resp_rows(kp0));
@@ -288,9 +292,10 @@ int sm_count()
     return sms > 0 ? sms : 1;
 }
 
-int launch_stream(pado_op_s *op, const StreamParams &sp, int threads, size_t smem, int ctas_per_sm, cudaStream_t st)
+int launch_stream(pado_op_s *op, const StreamParams &sp, bool adj, int threads, size_t smem, int ctas_per_sm,
+                  cudaStream_t st)
 {
-    StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1, sp.kp.L);
+    StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1, sp.kp.L, adj);
     const long long grid = std::min<long long>(sp.ntiles, (long long)ctas_per_sm * sm_count());
     if (grid < 1) return PADO_OK;
     fn<<<(unsigned)grid, threads, smem, st>>>(sp);
@@ -363,14 +368,14 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
                                          : cudaMemsetAsync(df, 0, total * sizeof(double), st);
         return e == cudaSuccess ? PADO_OK : cuda_fail(e);
     }
-    if (!adjoint && (op->variant == 0 || op->variant == 4)) {
+    if (op->variant == 0 || op->variant == 4) {
         const bool bounded_bc = !op->periodic && op->scheme != CD06;
-        const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, 0));
+        const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, adjoint ? 1 : 0));
         StreamParams sp;
         int sthreads = 0, sctas = 0;
         size_t ssmem = 0;
-        if (plan_stream(op, dt, kp, axis, na, nb, &sp, &sthreads, &ssmem, &sctas))
-            return launch_stream(op, sp, sthreads, ssmem, sctas, st);
+        if (plan_stream(op, dt, kp, axis, na, nb, adjoint, &sp, &sthreads, &ssmem, &sctas))
+            return launch_stream(op, sp, adjoint, sthreads, ssmem, sctas, st);
         if (op->variant == 4) return PADO_E_UNSUPPORTED;
     }
     // lines per CTA: the handle's choice, halved until the segments fit
@@ -470,6 +475,10 @@ void pado_destroy(pado_op_t op)
     for (void *p : op->allocations) cudaFree(p);
     if (op->stage_f) cudaFree(op->stage_f);
     if (op->stage_df) cudaFree(op->stage_df);
+    for (cudaEvent_t ev : op->ev_in) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : op->ev_out) cudaEventDestroy(ev);
+    if (op->s_h2d) cudaStreamDestroy(op->s_h2d);
+    if (op->s_d2h) cudaStreamDestroy(op->s_d2h);
     if (op->d_status) cudaFree(op->d_status);
     delete op;
 }
@@ -509,28 +518,93 @@ int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, doub
 {
     if (!op) return PADO_E_NULL;
     if (na < 0 || nb < 0) return PADO_E_ARG;
+    if (axis < 1 || axis > 3) return PADO_E_ARG;
     const size_t total = (size_t)op->n * (size_t)na * (size_t)nb;
     if (total == 0) return PADO_OK;
     if (!f_host || !df_host) return PADO_E_NULL;
+    if (f_host == df_host) return PADO_E_ALIAS;
     cudaStream_t st = (cudaStream_t)stream;
     std::lock_guard<std::mutex> g(op->staging_mu);
-    if (op->stage_elems < total) {
+
+    // Chunks: groups of whole lines.  x lines: consecutive lines (contiguous);
+    // y lines: consecutive (.., .., k) slabs (contiguous); z lines: a range of
+    // the middle index, one strided 2-D copy per chunk.  Each chunk is solved
+    // as its own compact field, so its device base is rounded to 32 doubles.
+    const size_t n = (size_t)op->n;
+    const size_t units = axis == 1 ? (size_t)na * (size_t)nb : (size_t)nb;
+    const size_t unit_elems = total / units;
+    const size_t target = HOST_CHUNK_BYTES / sizeof(double);
+    size_t nch = std::min<size_t>(std::max<size_t>(1, (total + target - 1) / target), HOST_MAX_CHUNKS);
+    nch = std::min(nch, units);
+    const size_t per = (units + nch - 1) / nch;
+    nch = (units + per - 1) / per;
+    const size_t slot = (per * unit_elems + 31) / 32 * 32;
+    const size_t need = slot * nch;
+    if (op->stage_elems < need) {
         if (op->stage_f) cudaFree(op->stage_f);
         if (op->stage_df) cudaFree(op->stage_df);
         op->stage_f = op->stage_df = nullptr;
         op->stage_elems = 0;
-        cudaError_t e = cudaMalloc(&op->stage_f, total * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc(&op->stage_df, total * sizeof(double));
+        cudaError_t e = cudaMalloc(&op->stage_f, need * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&op->stage_df, need * sizeof(double));
         if (e != cudaSuccess) return cuda_fail(e);
-        op->stage_elems = total;
+        op->stage_elems = need;
     }
-    cudaError_t e = cudaMemcpyAsync(op->stage_f, f_host, total * sizeof(double), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_fail(e);
-    int rc = launch(op, kind, axis, op->stage_f, op->stage_df, na, nb, bc1, bcn, st, false);
+    if (!op->s_h2d) {
+        cudaError_t e = cudaStreamCreateWithFlags(&op->s_h2d, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&op->s_d2h, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(e);
+    }
+    while (op->ev_in.size() < nch) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        cudaError_t e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e);
+        op->ev_in.push_back(a);
+        op->ev_out.push_back(b);
+    }
+
+    auto copy = [&](size_t c, bool in, cudaStream_t cs) -> cudaError_t {
+        const size_t u0 = c * per, cu = std::min(per, units - u0);
+        double *dev = (in ? op->stage_f : op->stage_df) + c * slot;
+        if (axis == 3) {
+            // (na, nb, n): rows of na*cu doubles, one per z plane
+            const size_t w = (size_t)na * cu * sizeof(double), hp = (size_t)na * (size_t)nb * sizeof(double);
+            const size_t off = u0 * (size_t)na;
+            return in ? cudaMemcpy2DAsync(dev, w, f_host + off, hp, w, n, cudaMemcpyHostToDevice, cs)
+                      : cudaMemcpy2DAsync(df_host + off, hp, dev, w, w, n, cudaMemcpyDeviceToHost, cs);
+        }
+        const size_t off = u0 * unit_elems, bytes = cu * unit_elems * sizeof(double);
+        return in ? cudaMemcpyAsync(dev, f_host + off, bytes, cudaMemcpyHostToDevice, cs)
+                  : cudaMemcpyAsync(df_host + off, dev, bytes, cudaMemcpyDeviceToHost, cs);
+    };
+
+    int rc = PADO_OK;
+    cudaError_t e = cudaSuccess;
+    for (size_t c = 0; c < nch && e == cudaSuccess; ++c) {
+        e = copy(c, true, op->s_h2d);
+        if (e == cudaSuccess) e = cudaEventRecord(op->ev_in[c], op->s_h2d);
+    }
+    for (size_t c = 0; c < nch && e == cudaSuccess && rc == PADO_OK; ++c) {
+        const size_t cu = std::min(per, units - c * per);
+        const long ca = axis == 1 ? (long)cu : na, cb = axis == 1 ? 1L : (long)cu;
+        e = cudaStreamWaitEvent(st, op->ev_in[c], 0);
+        if (e != cudaSuccess) break;
+        rc = launch(op, kind, axis, op->stage_f + c * slot, op->stage_df + c * slot, ca, cb, bc1, bcn, st, false);
+        if (rc != PADO_OK) break;
+        e = cudaEventRecord(op->ev_out[c], st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(op->s_d2h, op->ev_out[c], 0);
+        if (e == cudaSuccess) e = copy(c, false, op->s_d2h);
+    }
+    // every copy that was enqueued ends before the host buffers are handed back
+    const cudaError_t e1 = cudaStreamSynchronize(op->s_h2d);
+    const cudaError_t e2 = cudaStreamSynchronize(op->s_d2h);
+    const cudaError_t e3 = cudaStreamSynchronize(st);
     if (rc != PADO_OK) return rc;
-    e = cudaMemcpyAsync(df_host, op->stage_df, total * sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    return e == cudaSuccess ? PADO_OK : cuda_fail(e);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (e1 != cudaSuccess) return cuda_fail(e1);
+    if (e2 != cudaSuccess) return cuda_fail(e2);
+    return e3 == cudaSuccess ? PADO_OK : cuda_fail(e3);
 }
 
 int pado_set_tiling(pado_op_t op, int m, int lines)
@@ -576,7 +650,7 @@ int pado_launch_plan(pado_op_t op, int kind, int axis, const double *f, double *
         StreamParams sp;
         int threads = 0, ctas = 0;
         size_t smem = 0;
-        if (plan_stream(op, dt, kp, axis, na, nb, &sp, &threads, &smem, &ctas)) {
+        if (plan_stream(op, dt, kp, axis, na, nb, false, &sp, &threads, &smem, &ctas)) {
             info[0] = 4;
             info[1] = sp.kp.L;
             info[2] = sp.stages;

@@ -455,10 +455,12 @@ inline RhsCoef make_rhs_coef(int scheme, int kind, double dx, int periodic)
 // Per banded row the device table holds 16 doubles (128 bytes):
 // ---------------------------------------------------------------------------
 // Staged per-row table of the streaming kernel: the fields its sweeps read,
-// pairs that are loaded together kept adjacent.
+// pairs that are loaded together kept adjacent.  The output scale delta of a
+// transposed sweep is not 1 only for tridiagonal sweeps, which have no
+// second lag: it shares the c2 slot (E_DELTA).
 enum EtabField {
     E_C1 = 0, E_C2 = 1, E_ALPHA = 2, E_K1 = 3, E_K2 = 4, E_D2 = 5, E_U = 6, E_V = 7, E_GAMMA = 8, E_D1 = 9,
-    E_S = 10, E_T = 11, E_NF = 12
+    E_S = 10, E_T = 11, E_NF = 12, E_DELTA = E_C2
 };
 
 enum TabField {

@@ -30,29 +30,30 @@ KernelFn pick_m(int m, bool adj, bool contiguous, int variant)
     }
 }
 
-template <bool PER, bool XL, int LT>
+template <bool PER, bool XL, int LT, bool ADJ>
 StreamFn pick_stream_m(int m)
 {
     constexpr int RK = 2;
     switch (m) {
-    case 16: return stream_kernel<RK, PER, 16, XL, LT>;
-    case 32: return stream_kernel<RK, PER, 32, XL, LT>;
-    default: return stream_kernel<RK, PER, 64, XL, LT>;
+    case 16: return stream_kernel<RK, PER, 16, XL, LT, ADJ>;
+    case 32: return stream_kernel<RK, PER, 32, XL, LT, ADJ>;
+    default: return stream_kernel<RK, PER, 64, XL, LT, ADJ>;
     }
 }
 
-template <bool PER>
+template <bool PER, bool ADJ>
 StreamFn pick_stream_l(int m, bool xl, int lines)
 {
-    if (xl) return pick_stream_m<PER, true, 0>(m);
-    return lines == 8 ? pick_stream_m<PER, false, 8>(m) : pick_stream_m<PER, false, 16>(m);
+    if (xl) return pick_stream_m<PER, true, 0, ADJ>(m);
+    return lines == 8 ? pick_stream_m<PER, false, 8, ADJ>(m) : pick_stream_m<PER, false, 16, ADJ>(m);
 }
 
 }  // namespace
 
-StreamFn pick_stream_rk2(bool per, int m, bool xl, int lines)
+StreamFn pick_stream_rk2(bool per, int m, bool xl, int lines, bool adj)
 {
-    return per ? pick_stream_l<true>(m, xl, lines) : pick_stream_l<false>(m, xl, lines);
+    if (adj) return per ? pick_stream_l<true, true>(m, xl, lines) : pick_stream_l<false, true>(m, xl, lines);
+    return per ? pick_stream_l<true, false>(m, xl, lines) : pick_stream_l<false, false>(m, xl, lines);
 }
 
 KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant)

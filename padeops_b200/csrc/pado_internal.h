@@ -57,6 +57,8 @@ struct pado_op_s {
     std::mutex staging_mu;
     double *stage_f = nullptr, *stage_df = nullptr;
     size_t stage_elems = 0;
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;  // copy streams of the host-buffer pipeline
+    std::vector<cudaEvent_t> ev_in, ev_out;          // per chunk: copied in / computed
 };
 
 namespace pado {
@@ -72,11 +74,11 @@ KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant
 KernelFn pick_kernel_rk3(bool per, bool adj, bool contiguous, int m, int variant);
 using StreamFn = void (*)(const StreamParams);
 // streaming kernels: strided lines are built for 8 or 16 lines per tile
-// (`lines`), x lines for any
-StreamFn pick_stream_rk0(bool per, int m, bool xl, int lines);
-StreamFn pick_stream_rk1(bool per, int m, bool xl, int lines);
-StreamFn pick_stream_rk2(bool per, int m, bool xl, int lines);
-StreamFn pick_stream_rk3(bool per, int m, bool xl, int lines);
+// (`lines`), x lines for any; adj: the adjoint (transposed sweep, then B^T)
+StreamFn pick_stream_rk0(bool per, int m, bool xl, int lines, bool adj);
+StreamFn pick_stream_rk1(bool per, int m, bool xl, int lines, bool adj);
+StreamFn pick_stream_rk2(bool per, int m, bool xl, int lines, bool adj);
+StreamFn pick_stream_rk3(bool per, int m, bool xl, int lines, bool adj);
 
 // no_fast: every segment on the per-row table (for kernels built for a
 // segment length other than the handle's).

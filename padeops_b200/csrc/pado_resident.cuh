@@ -19,17 +19,26 @@
 //           x -> the output line (global memory, or the tile)
 // Three barriers separate prep, fwd, bwd and fin: the chains run inside the
 // phases that use them.
+//
+// The adjoint (ADJ) solves A^T z = g with the transposed sweep tables: fwd
+// reads g from the tile (no stencil, no prep), fin writes z back into the
+// tile (scaled by the transposed sweep's delta), and adj_out applies B^T
+// (reversed interior taps; explicit columns at a bounded line's ends) from
+// the tile to the output after one more barrier.
 #pragma once
 
 #include "pado_kernels.cuh"
 
 namespace pado {
 
-template <int RK, bool PER, int M>
+template <int RK, bool PER, int M, bool ADJ = false>
 struct ResidentLine {
     static constexpr bool CYC = PER;
     static constexpr bool ORDER2 = RK != RHS_CD06_D1;
-    static constexpr bool HAS_ALPHA = RK == RHS_CD06_D1 && !PER;
+    // only the bounded cd06 (Thomas) sweep scales its input (alpha != 1), and
+    // only its adjoint scales the output (delta != 1)
+    static constexpr bool HAS_ALPHA = RK == RHS_CD06_D1 && !PER && !ADJ;
+    static constexpr bool HAS_DELTA = RK == RHS_CD06_D1 && !PER && ADJ;
     static constexpr int CR = (RK == RHS_CD06_D1 || RK == RHS_CD10_D2) ? 3 : 4;  // closure_rows(RK)
     using LK = LineKernel<RK, PER, false, M, IN_ROWS>;
 
@@ -88,8 +97,10 @@ struct ResidentLine {
     static PADO_HD PADO_INLINE void fwd_fast(const KParams &kp, const Smem &sm, double *p, long long rs, int l, int s,
                                              int a, double (&w)[9], const Halo &h)
     {
+        if (!ADJ) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) w[4 + k] = p[(long long)k * rs];
+            for (int k = 0; k < 5; ++k) w[4 + k] = p[(long long)k * rs];
+        }
         const double al = kp.kc[0], c1 = kp.kc[1], c2 = kp.kc[2];
         double cst[5];
 #pragma unroll
@@ -99,7 +110,7 @@ struct ResidentLine {
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
 #pragma unroll
         for (int t = 0; t < M; ++t) {
-            double z = rhs_interior_fma(RK, PER, cst, w);
+            double z = ADJ ? p[(long long)t * rs] : rhs_interior_fma(RK, PER, cst, w);
             if (HAS_ALPHA) z *= al;
             if (ORDER2) z -= c2 * z2;
             z -= c1 * z1;
@@ -111,10 +122,12 @@ struct ResidentLine {
             }
             z2 = z1;
             z1 = z;
+            if (!ADJ) {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
-            if (t + 5 < M) w[8] = p[(long long)(t + 5) * rs];
-            else if (t + 5 - M < 4) w[8] = h.hn[t + 5 - M];
+                for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
+                if (t + 5 < M) w[8] = p[(long long)(t + 5) * rs];
+                else if (t + 5 - M < 4) w[8] = h.hn[t + 5 - M];
+            }
         }
         LK::template summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, s1, s2);
     }
@@ -155,8 +168,10 @@ struct ResidentLine {
         const int lenb = (a + len <= nb) ? len : nb - a;
         double *p = line + (long long)a * rs;
         double w[9];
+        if (!ADJ) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) w[k] = h.hp[k];
+            for (int k = 0; k < 4; ++k) w[k] = h.hp[k];
+        }
         double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0;
         if (fast(kp, s)) {
             // len == M, every window row inside the line; the spike terms of
@@ -166,8 +181,10 @@ struct ResidentLine {
             else fwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, w, h);
             return;
         }
+        if (!ADJ) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) w[4 + k] = k < len ? p[(long long)k * rs] : pick4(h.hn, k - len);
+            for (int k = 0; k < 5; ++k) w[4 + k] = k < len ? p[(long long)k * rs] : pick4(h.hn, k - len);
+        }
         const double *tb = seg_etab(sm, s);
         const bool first = !PER && s == 0, last = !PER && s == kp.S - 1;
         double rb0 = 0.0, rb1 = 0.0;
@@ -178,9 +195,14 @@ struct ResidentLine {
         for (int k = 0; k < 5; ++k) cst[k] = kp.rc.c[k];
 #pragma unroll 8
         for (int t = 0; t < len; ++t) {
-            double r = rhs_interior(RK, PER, cst, w);
-            if (first && t < CR) r = pick4(h.cv, t);
-            if (last && a + t >= n - CR) r = pick4(h.cl, a + t - (n - CR));
+            double r;
+            if (ADJ) {
+                r = p[(long long)t * rs];
+            } else {
+                r = rhs_interior(RK, PER, cst, w);
+                if (first && t < CR) r = pick4(h.cv, t);
+                if (last && a + t >= n - CR) r = pick4(h.cl, a + t - (n - CR));
+            }
             if (t < lenb) {
                 const double *tr = tb + (size_t)t * E_NF;
                 const Dbl2 cc = tld2<STAGED>(tr + E_C1);
@@ -200,11 +222,13 @@ struct ResidentLine {
                 if (t == lenb) rb0 = r;
                 else rb1 = r;
             }
+            if (!ADJ) {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
-            const int nx = t + 5;
-            if (nx < len) w[8] = p[(long long)nx * rs];
-            else if (nx - len < 4) w[8] = pick4(h.hn, nx - len);
+                for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
+                const int nx = t + 5;
+                if (nx < len) w[8] = p[(long long)nx * rs];
+                else if (nx - len < 4) w[8] = pick4(h.hn, nx - len);
+            }
         }
         LK::template summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, s1, s2);
         if (CYC && s == kp.S - 1) {
@@ -351,6 +375,7 @@ struct ResidentLine {
                 x += E1 * rr[0];
                 if (ORDER2) x += E2 * rr[1];
             }
+            if (HAS_DELTA) x *= kp.kc[6];
             q[(long long)t * os] = x;
         }
     }
@@ -391,11 +416,115 @@ struct ResidentLine {
                 x += E1 * rr[0];
                 if (ORDER2) x += E2 * rr[1];
             }
+            if (HAS_DELTA) x *= tld<STAGED>(tb + (size_t)t * E_NF + E_DELTA);
             q[(long long)t * os] = x;
         }
         if (CYC && s == kp.S - 1) {
             out[(long long)nb * os] = sm.eb[(size_t)l * 4 + 0];
             if (kp.nbord == 2) out[(long long)(nb + 1) * os] = sm.eb[(size_t)l * 4 + 1];
+        }
+    }
+
+    // column j of B^T at a bounded line's end (explicit blocks; every row of
+    // the line when n <= 32), rows read with stride rs
+    static PADO_HD PADO_INLINE double bt_column(const double *bt, const double *line, long long rs, int n, int j)
+    {
+        double acc = 0.0;
+        if (n <= 32) {
+            const double *w = bt + (size_t)j * n;
+            for (int i = 0; i < n; ++i) acc += PADO_LDG(w + i) * line[(long long)i * rs];
+            return acc;
+        }
+        const int i0 = j < 8 ? 0 : n - 12;
+        const double *w = bt + (size_t)(j < 8 ? j : 8 + j - (n - 8)) * 12;
+        for (int i = 0; i < 12; ++i) acc += PADO_LDG(w + i) * line[(long long)(i0 + i) * rs];
+        return acc;
+    }
+
+    // ---- adjoint, in place (x lines: the tile then goes out by bulk copy) ----
+    // Columns of B^T at a bounded line's ends go through a small scratch: slot
+    // j (first columns) or zone + j - (n - zone) (last ones), zone = n <= 32 ?
+    // n : 8, value for line l at scratch[slot * L + l].
+    static PADO_HD PADO_INLINE int adj_scratch_slots(int n) { return n <= 32 ? n : 16; }
+    // phase A (z final in the tile): the 4 rows on each side of the segment,
+    // and the end columns of B^T among the segment's rows
+    static PADO_HD PADO_INLINE void adj_gather(const KParams &kp, const double *line, long long rs, int l, int s,
+                                               double *scratch, Halo &h)
+    {
+        const int n = kp.n, a = seg_start(kp, s), len = seg_len(kp, s);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            h.hp[k] = row_or_zero(line, rs, a - 4 + k, n);
+            h.hn[k] = row_or_zero(line, rs, a + len + k, n);
+        }
+        if (PER) return;
+        const int zone = n <= 32 ? n : 8;
+        for (int t = 0; t < len; ++t) {
+            const int j = a + t;
+            if (j < zone) scratch[(size_t)j * kp.L + l] = bt_column(kp.bt, line, rs, n, j);
+            else if (j >= n - zone && n > 32) scratch[(size_t)(8 + j - (n - 8)) * kp.L + l] = bt_column(kp.bt, line, rs, n, j);
+        }
+    }
+    // phase B (after a barrier): fbar = B^T z over the segment's rows, written
+    // over z; the 9-row window runs ahead of the writes
+    static PADO_HD PADO_INLINE void adj_inplace(const KParams &kp, double *line, long long rs, int l, int s,
+                                                const double *scratch, const Halo &h)
+    {
+        const int n = kp.n, a = seg_start(kp, s), len = seg_len(kp, s);
+        double tp[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tp[k] = kp.taps[k];
+        double *p = line + (long long)a * rs;
+        double w[9];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w[k] = h.hp[k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w[4 + k] = k < len ? p[(long long)k * rs] : pick4(h.hn, k - len);
+        const int zone = n <= 32 ? n : 8;
+        const bool edge = !PER && (a < zone || a + len > n - zone);
+#pragma unroll 4
+        for (int t = 0; t < len; ++t) {
+            const int nx = t + 4;
+            w[8] = nx < len ? p[(long long)nx * rs] : pick4(h.hn, nx - len);
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc += tp[k] * w[k];
+            const int j = a + t;
+            if (edge) {
+                if (j < zone) acc = scratch[(size_t)j * kp.L + l];
+                else if (j >= n - zone) acc = scratch[(size_t)(8 + j - (n - 8)) * kp.L + l];
+            }
+            p[(long long)t * rs] = acc;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
+        }
+    }
+
+    // ---- adjoint: fbar = B^T z, z in the tile (every segment's fin done) ----
+    static PADO_HD PADO_INLINE void adj_out(const KParams &kp, const double *line, long long rs, int s, double *out,
+                                            long long os, bool live)
+    {
+        if (!live) return;
+        const int n = kp.n, a = seg_start(kp, s), len = seg_len(kp, s);
+        double tp[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tp[k] = kp.taps[k];
+        double w[9];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) w[k] = row_or_zero(line, rs, a - 4 + k, n);
+        const int zone = n <= 32 ? n : 8;
+        const bool edge = !PER && (a < zone || a + len > n - zone);
+#pragma unroll 4
+        for (int t = 0; t < len; ++t) {
+            w[8] = row_or_zero(line, rs, a + t + 4, n);
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc += tp[k] * w[k];
+            const int j = a + t;
+            if (edge && (j < zone || j >= n - zone)) acc = bt_column(kp.bt, line, rs, n, j);
+            out[(long long)j * os] = acc;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
         }
     }
 };

@@ -232,11 +232,10 @@ __device__ __forceinline__ void stream_issue_load(const StreamParams &sp, double
 
 // LT: lines per tile for strided lines, fixed at compile time so that every
 // row offset in the [row][L] tile is an immediate (x lines: 0, L at run time)
-template <int RK, bool PER, int M, bool XL, int LT>
+template <int RK, bool PER, int M, bool XL, int LT, bool ADJ = false>
 __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ StreamParams sp)
 {
-    using K = LineKernel<RK, PER, false, M, IN_ROWS>;
-    using RL = ResidentLine<RK, PER, M>;
+    using RL = ResidentLine<RK, PER, M, ADJ>;
     extern __shared__ double smem_raw[];
     // 1024-byte aligned base, by pointer arithmetic on the shared array so
     // that the compiler keeps every access in the shared address space
@@ -312,15 +311,34 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
         stream_tile_origin(sp, t, &x0, &p0);
         const LineIO io = stream_line_io_at(sp, sm, l, x0, p0);
         typename RL::Halo h;
-        if (active) RL::prep(kp, line, rs, s, h);
-        __syncthreads();
+        if (!ADJ) {
+            if (active) RL::prep(kp, line, rs, s, h);
+            __syncthreads();
+        }
         if (active) RL::template fwd<true>(kp, sm, line, rs, l, s, h);
         __syncthreads();
         if (active) RL::template bwd<true>(kp, sm, line, rs, l, s);
         __syncthreads();
-        if (active) RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live);
+        // adjoint x lines: fbar over z in the tile, then the bulk stores, when
+        // the end columns of B^T fit the summary buffers (free after fin)
+        const bool adj_tile = ADJ && XL && (PER || RL::adj_scratch_slots(kp.n) <= 6 * S + 4);
+        if (ADJ) {
+            // z = A^{-T} g back into the tile, then fbar = B^T z
+            if (active) RL::template fin<true>(kp, sm, line, rs, l, s, line, rs, true);
+            __syncthreads();
+            if (adj_tile) {
+                if (active) RL::adj_gather(kp, line, rs, l, s, sm.buf4, h);
+                __syncthreads();
+                if (active) RL::adj_inplace(kp, line, rs, l, s, sm.buf4, h);
+            } else {
+                double *dst = XL ? kp.out + (io.live ? (x0 + l) * (long long)kp.n : 0) : io.dst;
+                if (active) RL::adj_out(kp, line, rs, s, dst, XL ? 1 : io.ds, io.live);
+            }
+        } else {
+            if (active) RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live);
+        }
         const long long tn = t + (long long)stages * G;  // tile for this buffer next
-        if (XL) {
+        if (XL && (!ADJ || adj_tile)) {
             // each line's results -> global memory, then the buffer takes the next load
             fence_proxy_async();
             __syncthreads();
@@ -341,11 +359,10 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
 
 // Host emulation (tests): the kernel's tile loop with plain copies standing
 // in for the tensor / bulk copies; phases in kernel order over all threads.
-template <int RK, bool PER, int M, bool XL>
+template <int RK, bool PER, int M, bool XL, bool ADJ = false>
 inline void emulate_stream(const StreamParams &sp, int nthreads)
 {
-    using K = LineKernel<RK, PER, false, M, IN_ROWS>;
-    using RL = ResidentLine<RK, PER, M>;
+    using RL = ResidentLine<RK, PER, M, ADJ>;
     const KParams &kp = sp.kp;
     const int L = kp.L, S = kp.S;
     const StreamLayout lay =
@@ -382,8 +399,11 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
                 else sm.tile[(size_t)r * L + ll] = kp.in[x0 + ll + p * sp.pstride + (long long)r * kp.stride];
             }
         }
+        const bool adj_tile = ADJ && XL && (PER || RL::adj_scratch_slots(kp.n) <= 6 * S + 4);
+        // phases in kernel order, a barrier between consecutive ones
         for (int ph = 0; ph < 6; ++ph) {
-            if (ph == 2 || ph == 4) continue;  // the chains run inside bwd and fin
+            if (ADJ ? ph == 0 : ph >= 4) continue;
+            if (ph == 5 && !adj_tile) continue;
             for (int tid = 0; tid < nthreads; ++tid) {
                 const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
                 if (slot >= S) continue;
@@ -392,14 +412,22 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
                 switch (ph) {
                 case 0: RL::prep(kp, line, rs, s, H[tid]); break;
                 case 1: RL::template fwd<true>(kp, sm, line, rs, l, s, H[tid]); break;
-                case 2: K::chain_fwd(kp, sm, l, s); break;
-                case 3: RL::template bwd<true>(kp, sm, line, rs, l, s); break;
-                case 4: K::chain_bwd(kp, sm, l, s); break;
-                default: RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live); break;
+                case 2: RL::template bwd<true>(kp, sm, line, rs, l, s); break;
+                case 3:
+                    if (ADJ) RL::template fin<true>(kp, sm, line, rs, l, s, line, rs, true);
+                    else RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live);
+                    break;
+                case 4:
+                    if (adj_tile) RL::adj_gather(kp, line, rs, l, s, sm.buf4, H[tid]);
+                    else
+                        RL::adj_out(kp, line, rs, s, XL ? kp.out + (io.live ? (x0 + l) * (long long)kp.n : 0) : io.dst,
+                                    XL ? 1 : io.ds, io.live);
+                    break;
+                default: RL::adj_inplace(kp, line, rs, l, s, sm.buf4, H[tid]); break;
                 }
             }
         }
-        if (XL)
+        if (XL && (!ADJ || adj_tile))
             for (int ll = 0; ll < nl; ++ll)
                 for (int r = 0; r < kp.n; ++r) kp.out[(x0 + ll) * kp.n + r] = sm.tile[(size_t)ll * kp.P + r];
     }

@@ -644,7 +644,7 @@ ChainTables chain_tables(const std::vector<double> &tab, const std::vector<doubl
     return ct;
 }
 
-void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, unsigned spk,
+void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, unsigned spk, bool tri,
                 std::vector<double> &etab, std::vector<double> &ktab, std::vector<int> &toff)
 {
     etab.clear();
@@ -659,7 +659,7 @@ void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsig
                 const double *r = &tab[(size_t)i * T_NF];
                 double e[E_NF];
                 e[E_C1] = r[T_C1];
-                e[E_C2] = r[T_C2];
+                e[E_C2] = tri ? r[T_DELTA] : r[T_C2];  // E_DELTA for tridiagonal sweeps
                 e[E_ALPHA] = r[T_ALPHA];
                 e[E_K1] = r[T_K1];
                 e[E_K2] = r[T_K2];
@@ -700,7 +700,8 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     ot.interior = interior_info(sw, ot.lay, m);
     ot.chain = chain_tables(ot.tab, segsum, ot.lay, sw.nb, ot.interior, m);
     ot.chain_exact = chain_tables(ot.tab, segsum, ot.lay, sw.nb, Interior{}, m);
-    edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask, ot.interior.spk_mask, ot.etab, ot.ktab, ot.toff);
+    edge_table(ot.tab, ot.lay, sw.nb, ot.interior.mask, ot.interior.spk_mask, ot.rc.rk == RHS_CD06_D1, ot.etab,
+               ot.ktab, ot.toff);
     if (sw.nbord > 0) {
         // backward sweep of the unit spike sources: x_i = -e_i - d1_i x_{i+1} - d2_i x_{i+2}
         const int nb = sw.nb;

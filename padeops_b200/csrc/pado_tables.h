@@ -106,9 +106,10 @@ ChainTables chain_tables(const std::vector<double> &tab, const std::vector<doubl
 // `mask`), packed in segment order (etab, the E_NF fields of EtabField per
 // row), and the cyclic sums' spike values (k1, k2) of the rows of the
 // segments in `spk` (ktab, 2 per row); toff[s] = first packed row of segment s
-// in its table (0 otherwise).
+// in its table (0 otherwise).  tri: a tridiagonal sweep, whose c2 slot
+// carries delta instead (E_DELTA).
 constexpr int KT_NF = 2;
-void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, unsigned spk,
+void edge_table(const std::vector<double> &tab, const Layout &lay, int nb, unsigned mask, unsigned spk, bool tri,
                 std::vector<double> &etab, std::vector<double> &ktab, std::vector<int> &toff);
 
 // Everything a kernel launch reads for one (scheme, kind, closures,

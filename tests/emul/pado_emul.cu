@@ -80,24 +80,30 @@ extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, 
 
 // The streaming kernel's tile loop (primal): tiles of `lines` lines, x
 // lines through the [L][n+2] tile, y/z lines through the [row][L] tile.
-template <int RK, bool PER>
-static int stream_pick(const StreamParams &sp, int m, bool xl, int nthreads)
+template <int RK, bool PER, bool ADJ>
+static int stream_pick_adj(const StreamParams &sp, int m, bool xl, int nthreads)
 {
     switch (m * 2 + (xl ? 1 : 0)) {
-    case 32: emulate_stream<RK, PER, 16, false>(sp, nthreads); return 0;
-    case 33: emulate_stream<RK, PER, 16, true>(sp, nthreads); return 0;
-    case 64: emulate_stream<RK, PER, 32, false>(sp, nthreads); return 0;
-    case 65: emulate_stream<RK, PER, 32, true>(sp, nthreads); return 0;
-    case 128: emulate_stream<RK, PER, 64, false>(sp, nthreads); return 0;
-    case 129: emulate_stream<RK, PER, 64, true>(sp, nthreads); return 0;
+    case 32: emulate_stream<RK, PER, 16, false, ADJ>(sp, nthreads); return 0;
+    case 33: emulate_stream<RK, PER, 16, true, ADJ>(sp, nthreads); return 0;
+    case 64: emulate_stream<RK, PER, 32, false, ADJ>(sp, nthreads); return 0;
+    case 65: emulate_stream<RK, PER, 32, true, ADJ>(sp, nthreads); return 0;
+    case 128: emulate_stream<RK, PER, 64, false, ADJ>(sp, nthreads); return 0;
+    case 129: emulate_stream<RK, PER, 64, true, ADJ>(sp, nthreads); return 0;
     }
     return -1;
 }
 
-extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, int lines,
-                           int axis, const double *f, double *df, long na, long nb)
+template <int RK, bool PER>
+static int stream_pick(const StreamParams &sp, int m, bool xl, int nthreads, bool adj)
 {
-    const OpTables ot = make_op_tables(scheme, kind, n, dx, periodic, bc1, bcn, m, false);
+    return adj ? stream_pick_adj<RK, PER, true>(sp, m, xl, nthreads) : stream_pick_adj<RK, PER, false>(sp, m, xl, nthreads);
+}
+
+extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, int lines,
+                           int axis, const double *f, double *df, long na, long nb, int adjoint)
+{
+    const OpTables ot = make_op_tables(scheme, kind, n, dx, periodic, bc1, bcn, m, adjoint != 0);
     const Layout &lay = ot.lay;
     StreamParams sp;
     std::memset(&sp, 0, sizeof(sp));
@@ -110,6 +116,7 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
     kp.tab = ot.tab.data();
     kp.ctab = ot.chain.ctab.data();
     kp.xtab = ot.chain.xtab.data();
+    kp.bt = ot.bt.empty() ? nullptr : ot.bt.data();
     const bool xl = axis == 1;
     sp.axis = axis;
     sp.stages = 1;
@@ -136,13 +143,13 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
     const bool per = periodic != 0;
     switch (ot.rc.rk) {
     case RHS_CD06_D1:
-        return per ? stream_pick<RHS_CD06_D1, true>(sp, m, xl, nthreads) : stream_pick<RHS_CD06_D1, false>(sp, m, xl, nthreads);
+        return per ? stream_pick<RHS_CD06_D1, true>(sp, m, xl, nthreads, adjoint) : stream_pick<RHS_CD06_D1, false>(sp, m, xl, nthreads, adjoint);
     case RHS_CD10_D1:
-        return per ? stream_pick<RHS_CD10_D1, true>(sp, m, xl, nthreads) : stream_pick<RHS_CD10_D1, false>(sp, m, xl, nthreads);
+        return per ? stream_pick<RHS_CD10_D1, true>(sp, m, xl, nthreads, adjoint) : stream_pick<RHS_CD10_D1, false>(sp, m, xl, nthreads, adjoint);
     case RHS_CD10_D2:
-        return per ? stream_pick<RHS_CD10_D2, true>(sp, m, xl, nthreads) : stream_pick<RHS_CD10_D2, false>(sp, m, xl, nthreads);
+        return per ? stream_pick<RHS_CD10_D2, true>(sp, m, xl, nthreads, adjoint) : stream_pick<RHS_CD10_D2, false>(sp, m, xl, nthreads, adjoint);
     default:
-        return per ? stream_pick<RHS_CF90, true>(sp, m, xl, nthreads) : stream_pick<RHS_CF90, false>(sp, m, xl, nthreads);
+        return per ? stream_pick<RHS_CF90, true>(sp, m, xl, nthreads, adjoint) : stream_pick<RHS_CF90, false>(sp, m, xl, nthreads, adjoint);
     }
 }
 

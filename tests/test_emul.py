@@ -27,7 +27,7 @@ def emul():
 
     lib = ctypes.CDLL(build())
     P, I, D, Lg = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
-    lib.emul_stream.argtypes = [I, I, I, D, I, I, I, I, I, I, P, P, Lg, Lg]
+    lib.emul_stream.argtypes = [I, I, I, D, I, I, I, I, I, I, P, P, Lg, Lg, I]
     lib.emul_apply.argtypes = [I, I, I, D, I, I, I, I, I, I, I, I, P, P, Lg, Lg, I]
     return lib
 
@@ -58,7 +58,7 @@ def test_stream_kernel_emulated(emul, scheme, kind, periodic):
                 ref = op.apply(kind, axis, f, na, nb, bc1, bcn).reshape(f.shape)
                 out = np.full_like(f, np.nan)
                 rc = emul.emul_stream(scheme, kind, n, dx, int(periodic), bc1, bcn, m, lines, axis,
-                                      f.ctypes.data, out.ctypes.data, na, nb)
+                                      f.ctypes.data, out.ctypes.data, na, nb, 0)
                 assert rc == 0
                 assert _rel(out, ref) <= 1e-12, (n, m, lines, bc1, bcn, axis, _rel(out, ref))
 
@@ -100,3 +100,26 @@ def test_adjoint_emulated(emul, scheme, kind, periodic):
                                      g.ctypes.data, out.ctypes.data, na, nb, fast)
                 assert rc == 0
                 assert _rel(out, ref) <= 1e-11, (n, m, bc1, bcn, axis, fast, _rel(out, ref))
+
+
+@pytest.mark.parametrize("scheme,kind", OPS)
+@pytest.mark.parametrize("periodic", [True, False])
+def test_stream_adjoint_emulated(emul, scheme, kind, periodic):
+    """The streaming kernel's adjoint (transposed sweep in the tile, then B^T)
+    equals D^T from the dense assembly."""
+    rng = np.random.default_rng(23 + scheme + 5 * kind)
+    # (32, 32) and (64, 64): one segment, too few summary slots for the end
+    # columns, so x lines store straight to global memory
+    for n, m, lines in [(10, 32, 16), (32, 32, 16), (33, 16, 8), (64, 64, 8), (100, 32, 16), (256, 32, 16)]:
+        for bc1, bcn in _bcs(scheme, periodic):
+            dx = 0.37
+            Dm = dense.operator(scheme, kind, n, dx, periodic, bc1, bcn)
+            for axis in (1, 2, 3):
+                g = rng.standard_normal(_shape(n, axis))
+                na, nb = [s for a, s in enumerate(g.shape[::-1]) if a != axis - 1]
+                ref = dense.apply_axis(Dm.T, g, axis)
+                out = np.full_like(g, np.nan)
+                rc = emul.emul_stream(scheme, kind, n, dx, int(periodic), bc1, bcn, m, lines, axis,
+                                      g.ctypes.data, out.ctypes.data, na, nb, 1)
+                assert rc == 0
+                assert _rel(out, ref) <= 1e-11, (n, m, lines, bc1, bcn, axis, _rel(out, ref))

@@ -111,3 +111,35 @@ def test_autograd_vs_dense_transpose():
     rr = dense.apply_axis(Dx, u0, 1) + dense.apply_axis(Dz, u0, 3) - g0
     ref = dense.apply_axis(Dx.T, rr, 1) + dense.apply_axis(Dz.T, rr, 3)
     assert rel_err(u.grad.cpu().numpy(), ref) <= 1e-11
+
+
+@pytest.mark.parametrize("scheme,kind", OPS)
+@pytest.mark.parametrize("periodic", [True, False])
+def test_stream_adjoint_vs_dense(scheme, kind, periodic):
+    """The streaming kernel's adjoint (variant 4: transposed sweep in the tile,
+    then B^T) against the dense D^T, every axis, lengths with one or many
+    segments and partial tiles; the line kernel's adjoint (variant 1) on the
+    same inputs agrees too."""
+    import torch
+
+    rng = np.random.default_rng(31 + scheme + 5 * kind)
+    for n in (10, 34, 100, 256, 512):
+        dx = 0.3
+        op = _make(scheme, n, dx, periodic)
+        bcs = [(0, 0)] if (periodic or scheme == oracle.CD06) else [(0, 0), (1, -1), (-1, 1), (1, 1)]
+        for bc1, bcn in bcs:
+            D = dense.operator(scheme, kind, n, dx, periodic, bc1, bcn)
+            for axis in (1, 2, 3):
+                shape = {1: (3, 5, n), 2: (3, n, 38), 3: (n, 3, 22)}[axis]
+                g = rng.standard_normal(shape)
+                na, nb = na_nb(shape, axis)
+                gt = torch.from_numpy(g).cuda()
+                ref = dense.apply_axis(D.T, g, axis)
+                for variant in (4, 1):
+                    op.set_variant(variant)
+                    out = torch.full_like(gt, float("nan"))
+                    op.apply(kind, axis, gt, out, na, nb, bc1, bcn, adjoint=True)
+                    torch.cuda.synchronize()
+                    assert op.device_status() == 0
+                    assert rel_err(out.cpu().numpy(), ref) <= 1e-11, (n, bc1, bcn, axis, variant)
+                op.set_variant(0)
