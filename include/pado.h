@@ -179,10 +179,11 @@ int pado_batch_run(pado_batch_t batch, void *stream);
 int pado_batch_run_loop(pado_batch_t batch, void *stream);
 /* Capture pado_batch_run into a CUDA graph once and replay it on `stream`. */
 int pado_batch_run_graph(pado_batch_t batch, void *stream);
-/* Launch shape of the persistent kernel: threads per CTA (128/256/512, 0 =
- * keep) and a cap on resident CTAs per SM (0 = as many as fit).  Used by the
- * autotuner; drops any captured graph. */
-int pado_batch_set_config(pado_batch_t batch, int threads, int ctas_per_sm);
+/* Launch shape of the persistent kernel: lines per tile (8/16/32/64; 0 =
+ * enough lines to keep every thread of the CTA busy, 384 / segments per line,
+ * within the shared-memory cap) and a cap on resident CTAs per SM (0 = as
+ * many as fit).  Used by the autotuner; drops any captured graph. */
+int pado_batch_set_config(pado_batch_t batch, int lines, int ctas_per_sm);
 /* Tiles, grid size, threads per CTA and dynamic shared memory of the batch. */
 int pado_batch_info(pado_batch_t batch, long long *ntiles, int *grid, int *threads, long long *smem_bytes);
 void pado_batch_destroy(pado_batch_t batch);

@@ -50,8 +50,9 @@ class Batch:
         """One launch per item (the per-field loop the batch replaces)."""
         check(L.lib().pado_batch_run_loop(self._h, self._stream()), "pado_batch_run_loop")
 
-    def set_config(self, threads: int = 0, ctas_per_sm: int = 0) -> int:
-        return L.lib().pado_batch_set_config(self._h, threads, ctas_per_sm)
+    def set_config(self, lines: int = 0, ctas_per_sm: int = 0) -> int:
+        """Lines per tile (8, 16, 32, 64; 0 = automatic) and a cap on CTAs per SM (0 = none)."""
+        return L.lib().pado_batch_set_config(self._h, lines, ctas_per_sm)
 
     def info(self) -> dict:
         nt, grid, thr, smem = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()

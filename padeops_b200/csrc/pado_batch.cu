@@ -16,10 +16,11 @@ struct pado_batch_s {
     std::vector<pado_batch_item> items;  // as given
     std::vector<BatchItemDev> dev;       // sorted most expensive tile first
     BatchItemDev *d_items = nullptr;
+    long long *d_tile0s = nullptr;            // first tile of each item (compact copy for the search)
     unsigned long long *d_counter = nullptr;  // tile counter (device scratch)
     long long ntiles = 0;
     size_t smem = 0;
-    int threads = 256, ctas_per_sm = 0;
+    int lines = 0, ctas_per_sm = 0;  // lines per tile (0: 16 where it fits, else 8); CTA cap per SM
     int device = 0, num_sms = 0, grid = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -30,54 +31,94 @@ namespace {
 
 constexpr size_t BATCH_SMEM_CAP = 110 * 1024;  // per CTA, leaves room for 2 CTAs/SM
 
+}  // namespace
+
+namespace pado {
+
+// Descriptor of one item, with the tiling rules shared by batch objects and
+// the allocation-free launch.  lines: lines per tile (8, 16, 32 or 64), or 0:
+// as many as keep all BATCH_THREADS threads busy (BATCH_THREADS / segments,
+// a multiple of 8, at most 64) within the shared-memory cap -- short lines
+// have few segments, so their tiles take more lines.  *skip: nothing to do.
+int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d, long long *tiles, double *cost,
+                          size_t *smem, bool *skip)
+{
+    *skip = false;
+    if (!it.op) return PADO_E_NULL;
+    if (it.op->m != 16 && it.op->m != 32) return PADO_E_SIZE;  // batch kernels are built for 16- and 32-row segments
+    if (it.axis < 1 || it.axis > 3 || it.n1 < 0 || it.n2 < 0 || it.n3 < 0) return PADO_E_ARG;
+    const long long ext[3] = {it.n1, it.n2, it.n3};
+    if (ext[it.axis - 1] != it.op->n) return PADO_E_ARG;
+    const long long na = it.axis == 1 ? it.n2 : it.n1;
+    const long long nb = it.axis == 3 ? it.n2 : it.n3;
+    KParams kp;
+    bool trivial = true;
+    int rc = prepare_launch(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, false, 1, false,
+                            &kp, &trivial);
+    if (rc != PADO_OK) return rc;
+    if (trivial) {
+        if (it.op->n == 1 && (long long)na * nb > 0) return PADO_E_UNSUPPORTED;  // n == 1 items: use pado_apply
+        *skip = true;
+        return PADO_OK;
+    }
+    const bool xl = it.axis == 1;
+    const bool bounded_bc = !it.op->periodic && it.op->scheme != CD06;
+    const auto tit = it.op->tables.find(TabKey(it.kind, bounded_bc ? it.bc1 : 0, bounded_bc ? it.bcn : 0, 0));
+    if (tit == it.op->tables.end()) return PADO_E_STATE;
+    const DevTables &dt = tit->second;
+    const int erows = (int)(dt.host.etab.size() / E_NF), krows = (int)(dt.host.ktab.size() / KT_NF);
+    auto bytes = [&](int L_) {
+        return batch_smem_doubles(L_, kp.S, kp.n, xl, kp.xd, erows, krows, resp_rows(kp)) * sizeof(double);
+    };
+    int L = lines ? lines : std::min(64, (BATCH_THREADS / kp.S) & ~7);
+    if (L < 8 || L * kp.S > BATCH_THREADS) return PADO_E_SIZE;
+    while (L > 8 && bytes(L) > BATCH_SMEM_CAP) L -= 8;
+    if (bytes(L) > BATCH_SMEM_CAP) return PADO_E_SIZE;
+    kp.L = L;
+    std::memset(d, 0, sizeof(*d));
+    d->kp = kp;
+    d->etab = dt.etab;
+    d->ktab = dt.ktab;
+    d->rtab = dt.rtab;
+    d->toff = dt.toff;
+    d->code = batch_code(kp.rc.rk, it.op->periodic != 0, xl, it.op->m);
+    d->etab_rows = erows;
+    d->ktab_rows = krows;
+    *tiles = (kp.nlines + L - 1) / L;
+    *cost = (double)L * kp.n;
+    *smem = bytes(L);
+    return PADO_OK;
+}
+
+}  // namespace pado
+
+namespace {
+
 int layout_items(pado_batch_s *b)
 {
     struct Pre {
         BatchItemDev d;
+        long long tiles;
         double cost;
     };
     std::vector<Pre> pre;
     size_t smem = 0;
     for (const pado_batch_item &it : b->items) {
-        if (!it.op) return PADO_E_NULL;
-        if (it.op->m > BATCH_M) return PADO_E_SIZE;
-        if (it.axis < 1 || it.axis > 3 || it.n1 < 0 || it.n2 < 0 || it.n3 < 0) return PADO_E_ARG;
-        const long long ext[3] = {it.n1, it.n2, it.n3};
-        if (ext[it.axis - 1] != it.op->n) return PADO_E_ARG;
-        const long long na = it.axis == 1 ? it.n2 : it.n1;
-        const long long nb = it.axis == 3 ? it.n2 : it.n3;
-        const int P = (it.op->n % 2 == 0) ? it.op->n + 1 : it.op->n;
-        KParams kp;
-        bool trivial = true;
-        // the register-only path assumes segments of BATCH_M rows
-        int rc = prepare_launch(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, false, 1,
-                                it.op->m != BATCH_M, &kp, &trivial);
+        Pre p;
+        size_t sm = 0;
+        bool skip = false;
+        const int rc = batch_item_descriptor(it, b->lines, &p.d, &p.tiles, &p.cost, &sm, &skip);
         if (rc != PADO_OK) return rc;
-        if (trivial) {
-            if (it.op->n == 1 && (long long)na * nb > 0) return PADO_E_UNSUPPORTED;  // n == 1 items: use pado_apply
-            continue;
-        }
-        const int S = kp.S;
-        int L = b->threads / std::max(S, 1);
-        while (L > 1 && smem_doubles(L, S, kp.xd, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) --L;
-        if (L < 1 || smem_doubles(L, S, kp.xd, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) return PADO_E_SIZE;
-        kp.L = L;
-        Pre p{};
-        p.d.kp = kp;
-        p.d.code = kp.rc.rk * 4 + (it.op->periodic ? 2 : 0) + (kp.stride != 1 ? 1 : 0);
-        const long long tiles = (kp.nlines + L - 1) / L;
-        p.d.tile0 = tiles;  // temporarily the tile count
-        p.cost = (double)L * kp.n;
-        smem = std::max(smem, smem_doubles(L, kp.S, kp.xd, kp.stride == 1 ? (size_t)L * P : 0) * sizeof(double));
+        if (skip) continue;
+        smem = std::max(smem, sm);
         pre.push_back(p);
     }
     std::stable_sort(pre.begin(), pre.end(), [](const Pre &x, const Pre &y) { return x.cost > y.cost; });
     b->dev.clear();
     long long t0 = 0;
     for (Pre &p : pre) {
-        const long long tiles = p.d.tile0;
         p.d.tile0 = t0;
-        t0 += tiles;
+        t0 += p.tiles;
         b->dev.push_back(p.d);
     }
     b->ntiles = t0;
@@ -88,11 +129,17 @@ int layout_items(pado_batch_s *b)
 int upload_batch(pado_batch_s *b)
 {
     if (b->d_items) cudaFree(b->d_items);
+    if (b->d_tile0s) cudaFree(b->d_tile0s);
     b->d_items = nullptr;
+    b->d_tile0s = nullptr;
     if (!b->dev.empty()) {
+        std::vector<long long> t0(b->dev.size());
+        for (size_t i = 0; i < b->dev.size(); ++i) t0[i] = b->dev[i].tile0;
         cudaError_t e = cudaMalloc(&b->d_items, b->dev.size() * sizeof(BatchItemDev));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_tile0s, t0.size() * sizeof(long long));
         if (e != cudaSuccess) return cuda_fail(e);
         e = cudaMemcpy(b->d_items, b->dev.data(), b->dev.size() * sizeof(BatchItemDev), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b->d_tile0s, t0.data(), t0.size() * sizeof(long long), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return cuda_fail(e);
     }
     if (!b->d_counter) {
@@ -105,7 +152,7 @@ int upload_batch(pado_batch_s *b)
                                          (int)BATCH_SMEM_CAP);
     if (e != cudaSuccess) return cuda_fail(e);
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, b->threads, b->smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, BATCH_THREADS, b->smem);
     if (e != cudaSuccess) return cuda_fail(e);
     if (per_sm < 1) return PADO_E_SIZE;
     if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
@@ -128,7 +175,8 @@ int enqueue_persistent(pado_batch_s *b, cudaStream_t st)
     if (b->ntiles == 0) return PADO_OK;
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return cuda_fail(e);
-    batch_kernel<<<b->grid, b->threads, b->smem, st>>>(b->d_items, (int)b->dev.size(), b->ntiles, b->d_counter);
+    batch_kernel<<<b->grid, BATCH_THREADS, b->smem, st>>>(b->d_items, b->d_tile0s, (int)b->dev.size(), b->ntiles,
+                                                          b->d_counter);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     e = cudaGetLastError();
     return e == cudaSuccess ? PADO_OK : cuda_fail(e);
@@ -158,12 +206,12 @@ int pado_batch_create(pado_batch_t *out, const pado_batch_item *items, int nitem
     return PADO_OK;
 }
 
-int pado_batch_set_config(pado_batch_t b, int threads, int ctas_per_sm)
+int pado_batch_set_config(pado_batch_t b, int lines, int ctas_per_sm)
 {
     if (!b) return PADO_E_NULL;
-    if (threads != 0 && threads != 128 && threads != 256 && threads != 512) return PADO_E_ARG;
+    if (lines != 0 && lines != 8 && lines != 16 && lines != 32 && lines != 64) return PADO_E_ARG;
     if (ctas_per_sm < 0) return PADO_E_ARG;
-    if (threads) b->threads = threads;
+    b->lines = lines;
     b->ctas_per_sm = ctas_per_sm;
     drop_graph(b);
     int rc = layout_items(b);
@@ -224,6 +272,7 @@ void pado_batch_destroy(pado_batch_t b)
     drop_graph(b);
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
     if (b->d_items) cudaFree(b->d_items);
+    if (b->d_tile0s) cudaFree(b->d_tile0s);
     if (b->d_counter) cudaFree(b->d_counter);
     delete b;
 }
@@ -232,20 +281,22 @@ void pado_batch_destroy(pado_batch_t b)
 
 // ---- the batched launch without device allocation --------------------------
 //
-// g_static_batch holds the tile counter (first 256 bytes) and the item
-// descriptors.  Host code must not use its name as an address: the device
-// address comes from cudaGetSymbolAddress, once per device.
+// g_static_batch holds the tile counter (first 256 bytes), the item
+// descriptors and their first tiles.  Host code must not use its name as an
+// address: the device address comes from cudaGetSymbolAddress, once per
+// device.
 
 namespace {
 
 constexpr size_t STATIC_ITEMS_OFFSET = 256;
-static_assert(STATIC_ITEMS_OFFSET + (size_t)PADO_STATIC_BATCH_MAX_ITEMS * sizeof(BatchItemDev) <=
+constexpr size_t STATIC_TILE0_OFFSET = STATIC_ITEMS_OFFSET + (size_t)PADO_STATIC_BATCH_MAX_ITEMS * sizeof(BatchItemDev);
+static_assert(STATIC_TILE0_OFFSET % sizeof(long long) == 0, "tile start alignment");
+static_assert(STATIC_TILE0_OFFSET + (size_t)PADO_STATIC_BATCH_MAX_ITEMS * sizeof(long long) <=
                   (size_t)PADO_STATIC_BATCH_SCRATCH_BYTES,
               "static batch scratch too small for its item limit");
 static_assert(alignof(BatchItemDev) <= STATIC_ITEMS_OFFSET, "descriptor alignment");
 
 constexpr int STATIC_MAX_DEVICES = 64;
-constexpr int STATIC_THREADS = 256;  // threads per CTA (the batch object's default)
 constexpr int STATIC_CHUNK = 8;      // descriptors staged per host-to-device copy
 
 std::mutex g_static_mu;
@@ -269,45 +320,6 @@ int static_scratch(int dev, unsigned char **out)
         g_static_addr[dev] = static_cast<unsigned char *>(p);
     }
     *out = g_static_addr[dev];
-    return PADO_OK;
-}
-
-// One item's descriptor with the same tiling rules as a batch object
-// (STATIC_THREADS threads per CTA).  *skip: nothing to do for this item.
-int static_item(const pado_batch_item &it, int dev, BatchItemDev *d, long long *tiles, double *cost, size_t *smem,
-                bool *skip)
-{
-    *skip = false;
-    if (!it.op) return PADO_E_NULL;
-    if (it.op->device != dev) return PADO_E_ARG;
-    if (it.op->m > BATCH_M) return PADO_E_SIZE;
-    if (it.axis < 1 || it.axis > 3 || it.n1 < 0 || it.n2 < 0 || it.n3 < 0) return PADO_E_ARG;
-    const long long ext[3] = {it.n1, it.n2, it.n3};
-    if (ext[it.axis - 1] != it.op->n) return PADO_E_ARG;
-    const long long na = it.axis == 1 ? it.n2 : it.n1;
-    const long long nb = it.axis == 3 ? it.n2 : it.n3;
-    const int P = (it.op->n % 2 == 0) ? it.op->n + 1 : it.op->n;
-    KParams kp;
-    bool trivial = true;
-    int rc = prepare_launch(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, false, 1,
-                            it.op->m != BATCH_M, &kp, &trivial);
-    if (rc != PADO_OK) return rc;
-    if (trivial) {
-        if (it.op->n == 1 && (long long)na * nb > 0) return PADO_E_UNSUPPORTED;  // n == 1 items: use pado_apply
-        *skip = true;
-        return PADO_OK;
-    }
-    const int S = kp.S;
-    int L = STATIC_THREADS / std::max(S, 1);
-    while (L > 1 && smem_doubles(L, S, kp.xd, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) --L;
-    if (L < 1 || smem_doubles(L, S, kp.xd, (size_t)L * P) * sizeof(double) > BATCH_SMEM_CAP) return PADO_E_SIZE;
-    kp.L = L;
-    std::memset(d, 0, sizeof(*d));
-    d->kp = kp;
-    d->code = kp.rc.rk * 4 + (it.op->periodic ? 2 : 0) + (kp.stride != 1 ? 1 : 0);
-    *tiles = (kp.nlines + L - 1) / L;
-    *cost = (double)L * kp.n;
-    *smem = smem_doubles(L, kp.S, kp.xd, kp.stride == 1 ? (size_t)L * P : 0) * sizeof(double);
     return PADO_OK;
 }
 
@@ -337,7 +349,8 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
     for (int i = 0; i < nitems; ++i) {
         bool skip = false;
         size_t sm = 0;
-        rc = static_item(items[i], dev, &chunk[0], &tiles[i], &cost[i], &sm, &skip);
+        if (items[i].op && items[i].op->device != dev) return PADO_E_ARG;
+        rc = batch_item_descriptor(items[i], 0, &chunk[0], &tiles[i], &cost[i], &sm, &skip);
         if (rc != PADO_OK) return rc;
         if (skip) continue;
         smem = std::max(smem, sm);
@@ -355,6 +368,8 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
     cudaStream_t st = (cudaStream_t)stream;
     BatchItemDev *d_items = reinterpret_cast<BatchItemDev *>(base + STATIC_ITEMS_OFFSET);
     unsigned long long *d_counter = reinterpret_cast<unsigned long long *>(base);
+    long long *d_tile0s = reinterpret_cast<long long *>(base + STATIC_TILE0_OFFSET);
+    long long starts[PADO_STATIC_BATCH_MAX_ITEMS];
     long long t0 = 0;
     for (int k0 = 0; k0 < nvalid; k0 += STATIC_CHUNK) {
         const int kn = std::min(STATIC_CHUNK, nvalid - k0);
@@ -364,9 +379,10 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
             size_t sm = 0;
             long long nt = 0;
             double c = 0;
-            rc = static_item(items[i], dev, &chunk[k], &nt, &c, &sm, &skip);
+            rc = batch_item_descriptor(items[i], 0, &chunk[k], &nt, &c, &sm, &skip);
             if (rc != PADO_OK) return rc;
             chunk[k].tile0 = t0;
+            starts[k0 + k] = t0;
             t0 += nt;
         }
         // pageable source: the copy is staged before the call returns, so the
@@ -375,6 +391,8 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
         if (e != cudaSuccess) return cuda_fail(e);
     }
     const long long ntiles = t0;
+    e = cudaMemcpyAsync(d_tile0s, starts, (size_t)nvalid * sizeof(long long), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e);
     e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return cuda_fail(e);
 
@@ -382,13 +400,13 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
                              (int)BATCH_SMEM_CAP);
     if (e != cudaSuccess) return cuda_fail(e);
     int per_sm = 0, num_sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, STATIC_THREADS, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, BATCH_THREADS, smem);
     if (e != cudaSuccess) return cuda_fail(e);
     if (per_sm < 1) return PADO_E_SIZE;
     e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_fail(e);
     const long long grid = std::max<long long>(1, std::min<long long>((long long)per_sm * num_sms, ntiles));
-    batch_kernel<<<(unsigned)grid, STATIC_THREADS, smem, st>>>(d_items, nvalid, ntiles, d_counter);
+    batch_kernel<<<(unsigned)grid, BATCH_THREADS, smem, st>>>(d_items, d_tile0s, nvalid, ntiles, d_counter);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     e = cudaGetLastError();
     return e == cudaSuccess ? PADO_OK : cuda_fail(e);
@@ -399,7 +417,7 @@ int pado_batch_info(pado_batch_t b, long long *ntiles, int *grid, int *threads, 
     if (!b) return PADO_E_NULL;
     if (ntiles) *ntiles = b->ntiles;
     if (grid) *grid = b->grid;
-    if (threads) *threads = b->threads;
+    if (threads) *threads = BATCH_THREADS;
     if (smem_bytes) *smem_bytes = (long long)b->smem;
     return PADO_OK;
 }

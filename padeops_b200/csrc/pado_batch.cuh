@@ -1,67 +1,217 @@
 // pado_batch.cuh -- persistent kernel that runs many line families (fields of
 // uneven sizes, schemes, boundary types and directions) in one launch.
 //
-// Work unit = one tile (L lines of one field).  Tiles of all items are
-// numbered, most expensive item first; CTAs claim tiles from a device
-// counter (atomicAdd, no waiting on other CTAs) until the list is exhausted.
+// Work unit = one tile: L consecutive lines of one item (by default as many
+// as keep the CTA's 384 threads busy: 384 / segments per line), all rows,
+// resident in shared memory while
+// the tile-resident sweep of the streaming kernel (pado_resident.cuh) runs on
+// it.  Tiles of all items are numbered, most expensive item first; CTAs claim
+// tiles from a device counter (atomicAdd, no waiting on other CTAs) until the
+// list is exhausted.  Lines come in with plain coalesced loads (x lines: one
+// warp per line; y/z lines: L neighbouring lines per row), results leave
+// straight from the sweep (y/z) or from the tile (x).  The operator tables
+// are read from global memory (L1/L2 resident) instead of being staged: a
+// CTA meets a different item at every tile.
 #pragma once
 
 #include "pado_kernels.cuh"
+#include "pado_resident.cuh"
 
 namespace pado {
 
-constexpr int BATCH_M = 32;  // segment length of the batched kernel
+constexpr int BATCH_THREADS = 384;  // threads per CTA: lines per tile x segments per line
+#ifndef BATCH_MIN_CTAS
+#define BATCH_MIN_CTAS 2
+#endif
 
 struct BatchItemDev {
-    KParams kp;            // geometry, tables and tiling of this item
+    KParams kp;            // geometry and tiling of this item
+    const double *etab;    // per-row table of the edge segments
+    const double *ktab;    // spike rows of the cyclic sums
+    const double *rtab;    // border responses
+    const int *toff;       // first table row of each segment
     long long tile0;       // first tile index of this item
-    int code;              // rk * 4 + periodic * 2 + direct
-    int pad;
+    int code;              // ((rk * 2 + periodic) * 2 + x lines) * 2 + (segment length 32)
+    int etab_rows, ktab_rows, pad;
 };
 
-#ifdef __CUDACC__
-template <int RK, bool PER, bool STRIDED>
-__device__ __forceinline__ void batch_tile(const KParams &kp, double *smem, long long q0)
+PADO_HD PADO_INLINE int batch_code(int rk, bool periodic, bool xl, int m)
 {
-    const Smem sm = carve(smem, kp.L, kp.P, kp.S, kp.xd);
-    run_tile<RK, PER, false, BATCH_M, STRIDED ? IN_GLOBAL : IN_LINES>(kp, sm, q0);
+    return ((rk * 2 + (periodic ? 1 : 0)) * 2 + (xl ? 1 : 0)) * 2 + (m == 32 ? 1 : 0);
 }
 
-// counter: tile counter, zeroed before the launch.
-__global__ void __launch_bounds__(512) batch_kernel(const BatchItemDev *__restrict__ items, int nitems,
-                                                     long long ntiles, unsigned long long *counter)
+// Shared memory of a batch tile (doubles): the item's staged tables (etab,
+// ktab, rtab, toff), then the summaries, border slots, border weights,
+// transfer products and the tile (carve's layout).
+PADO_HD PADO_INLINE size_t batch_table_doubles(int S, int etab_rows, int ktab_rows, int resp_rows)
+{
+    return (size_t)etab_rows * E_NF + (size_t)ktab_rows * 2 + (size_t)resp_rows * 2 + (size_t)(S + 1) / 2;
+}
+PADO_HD PADO_INLINE size_t batch_smem_doubles(int L, int S, int n, bool xl, int xd, int etab_rows, int ktab_rows,
+                                              int resp_rows)
+{
+    return batch_table_doubles(S, etab_rows, ktab_rows, resp_rows) +
+           smem_doubles(L, S, xd, xl ? (size_t)L * (n | 1) : (size_t)L * n);
+}
+
+#ifdef __CUDACC__
+PADO_HD PADO_INLINE Smem batch_carve(const BatchItemDev &it, double *smem)
+{
+    const KParams &kp = it.kp;
+    double *p = smem;
+    double *etab = p;
+    p += (size_t)it.etab_rows * E_NF;
+    double *ktab = p;
+    p += (size_t)it.ktab_rows * 2;
+    double *rtab = p;
+    p += (size_t)resp_rows(kp) * 2;
+    int *toff = reinterpret_cast<int *>(p);
+    p += (size_t)(kp.S + 1) / 2;
+    Smem sm = carve(p, kp.L, 0, kp.S, kp.xd);
+    sm.etab = etab;
+    sm.ktab = ktab;
+    sm.rtab = rtab;
+    sm.toff = toff;
+    return sm;
+}
+
+// Copies the item's tables into its shared-memory slots (a CTA does this
+// only when its tile belongs to another item than its previous one).
+__device__ __forceinline__ void batch_stage(const BatchItemDev &it, const Smem &sm)
+{
+    const KParams &kp = it.kp;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    stage_chain_table(kp, sm, tid, nt);
+    double *etab = const_cast<double *>(sm.etab), *ktab = const_cast<double *>(sm.ktab);
+    double *rtab = const_cast<double *>(sm.rtab);
+    int *toff = const_cast<int *>(sm.toff);
+    for (int i = tid; i < it.etab_rows * E_NF; i += nt) etab[i] = __ldg(it.etab + i);
+    for (int i = tid; i < it.ktab_rows * 2; i += nt) ktab[i] = __ldg(it.ktab + i);
+    for (int i = tid; i < resp_rows(kp) * 2; i += nt) rtab[i] = __ldg(it.rtab + i);
+    for (int i = tid; i < kp.S; i += nt) toff[i] = __ldg(it.toff + i);
+}
+
+// One tile of one item (tables staged).  Not inlined: each (stencil,
+// boundary, direction, segment length) gets its own register allocation
+// instead of the kernel carrying the union of all of them.
+template <int RK, bool PER, int M, bool XL>
+__device__ __noinline__ void batch_tile(const BatchItemDev &it, double *smem, long long q0)
+{
+    using RL = ResidentLine<RK, PER, M>;
+    const KParams &kp = it.kp;
+    const int L = kp.L, S = kp.S, n = kp.n;
+    const int P = XL ? (n | 1) : n;  // odd pitch: the lanes (lines) of a warp hit different banks
+    const Smem sm = batch_carve(it, smem);
+    const int tid = threadIdx.x, nthreads = blockDim.x;
+    const long long rem = kp.nlines - q0;
+    const int nl = (int)(rem < L ? rem : L);
+
+    // load the tile (lines past the field's end read as zero)
+    if (XL) {
+        const int warp = tid >> 5, lane = tid & 31, nw = nthreads >> 5;
+        for (int l = warp; l < L; l += nw) {
+            const double *src = kp.in + (q0 + l) * (long long)n;
+            double *dst = sm.tile + (size_t)l * P;
+            for (int r = lane; r < n; r += 32) dst[r] = l < nl ? __ldcs(src + r) : 0.0;
+        }
+    } else {
+        const int l = tid % L, rstep = nthreads / L;
+        const double *src = kp.in + (l < nl ? line_base(kp, q0 + l) : 0);
+        for (int r = tid / L; r < n; r += rstep)
+            sm.tile[(size_t)r * L + l] = l < nl ? __ldcs(src + (long long)r * kp.stride) : 0.0;
+    }
+    __syncthreads();
+
+    const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
+    const bool active = slot < S;
+    const long long rs = XL ? 1 : (long long)L;
+    double *line = sm.tile + (XL ? (size_t)l * P : (size_t)l);
+    typename RL::Halo h;
+    if (active) RL::prep(kp, line, rs, s, h);
+    __syncthreads();
+    if (active) RL::template fwd<true>(kp, sm, line, rs, l, s, h);
+    __syncthreads();
+    if (active) RL::template bwd<true>(kp, sm, line, rs, l, s);
+    __syncthreads();
+    if (XL) {
+        if (active) RL::template fin<true>(kp, sm, line, rs, l, s, line, 1, true);
+        __syncthreads();
+        const int warp = tid >> 5, lane = tid & 31, nw = nthreads >> 5;
+        for (int ll = warp; ll < nl; ll += nw) {
+            double *dst = kp.out + (q0 + ll) * (long long)n;
+            const double *src = sm.tile + (size_t)ll * P;
+            for (int r = lane; r < n; r += 32) __stcs(dst + r, src[r]);
+        }
+    } else {
+        const bool live = l < nl;
+        double *dst = kp.out + (live ? line_base(kp, q0 + l) : 0);
+        if (active) RL::template fin<true>(kp, sm, line, rs, l, s, dst, kp.stride, live);
+    }
+}
+
+// items: descriptors in schedule order; tile0s[i] = items[i].tile0 (compact,
+// for the search); counter: tile counter, zeroed before the launch.
+__global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) batch_kernel(const BatchItemDev *__restrict__ items,
+                                                                 const long long *__restrict__ tile0s, int nitems,
+                                                                 long long ntiles, unsigned long long *counter)
 {
     extern __shared__ double smem_raw[];
     __shared__ long long s_tile;
+    __shared__ int s_last;
+    // the current item's descriptor, in shared memory: the sweeps read its
+    // parameters (segment starts, interior patterns) in their loops
+    __shared__ BatchItemDev s_it;
+    static_assert(sizeof(BatchItemDev) % sizeof(long long) == 0, "descriptor copy granularity");
+    if (threadIdx.x == 0) {
+        s_last = -1;
+        s_tile = (long long)atomicAdd(counter, 1ULL);
+    }
     for (;;) {
-        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(counter, 1ULL);
         __syncthreads();
         const long long t = s_tile;
-        __syncthreads();
         if (t >= ntiles) return;
         int lo = 0, hi = nitems - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].tile0 <= t) lo = mid;
+            if (__ldg(tile0s + mid) <= t) lo = mid;
             else hi = mid - 1;
         }
-        const BatchItemDev &it = items[lo];
-        const KParams &kp = it.kp;
-        const long long q0 = (t - it.tile0) * kp.L;
+        const bool fresh = lo != s_last;
+        if (fresh) {
+            const long long *src = reinterpret_cast<const long long *>(items + lo);
+            long long *dst = reinterpret_cast<long long *>(&s_it);
+            for (int i = threadIdx.x; i < (int)(sizeof(BatchItemDev) / sizeof(long long)); i += blockDim.x)
+                dst[i] = src[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_last = lo;
+            // claim the next tile now: the atomic's latency hides behind this one
+            s_tile = (long long)atomicAdd(counter, 1ULL);
+        }
+        if (fresh) {
+            batch_stage(s_it, batch_carve(s_it, smem_raw));
+            __syncthreads();
+        }
+        const BatchItemDev &it = s_it;
+        const long long q0 = (t - it.tile0) * it.kp.L;
         switch (it.code) {
-#define PADO_CASE(rk)                                                  \
-    case rk * 4 + 0: batch_tile<rk, false, false>(kp, smem_raw, q0); break; \
-    case rk * 4 + 1: batch_tile<rk, false, true>(kp, smem_raw, q0); break;  \
-    case rk * 4 + 2: batch_tile<rk, true, false>(kp, smem_raw, q0); break;  \
-    case rk * 4 + 3: batch_tile<rk, true, true>(kp, smem_raw, q0); break;
+#define PADO_CASE_M(rk, per, xl)                                                             \
+    case ((rk * 2 + per) * 2 + xl) * 2 + 0: batch_tile<rk, per, 16, xl>(it, smem_raw, q0); break; \
+    case ((rk * 2 + per) * 2 + xl) * 2 + 1: batch_tile<rk, per, 32, xl>(it, smem_raw, q0); break;
+#define PADO_CASE(rk)                  \
+    PADO_CASE_M(rk, false, false)      \
+    PADO_CASE_M(rk, false, true)       \
+    PADO_CASE_M(rk, true, false)       \
+    PADO_CASE_M(rk, true, true)
             PADO_CASE(0)
             PADO_CASE(1)
             PADO_CASE(2)
             PADO_CASE(3)
 #undef PADO_CASE
+#undef PADO_CASE_M
         default: break;
         }
-        __syncthreads();
     }
 }
 #endif

@@ -5,7 +5,7 @@ every legal (m, lines) tiling -- m = rows one thread sweeps serially (the
 Thomas part), n/m = segments joined by the inter-segment chain (the
 reduced/parallel part), lines = lines per CTA -- on a synthetic field of the
 caller's shape with CUDA events, and keeps the fastest.  For a batch it times
-the persistent kernel's threads-per-CTA / CTAs-per-SM choices.  Results are
+the persistent kernel's lines-per-tile / CTAs-per-SM choices.  Results are
 cached in a JSON file keyed by GPU name and problem signature
 (``$PADO_TUNE_CACHE`` or ``~/.cache/padeops_b200/tune.json``).
 """
@@ -114,11 +114,12 @@ def tune_op(op, kind: int, axis: int, shape: tuple[int, int, int], reps: int = 5
 
 
 def tune_batch(batch, reps: int = 5, verbose: bool = False) -> tuple[int, int, float]:
-    """Pick the persistent kernel's (threads per CTA, CTAs per SM) for a batch."""
+    """Pick the persistent kernel's (lines per tile, CTAs per SM) for a batch.
+    Returns (lines, ctas_per_sm, ms); 0 means automatic / no cap."""
     best = None
-    for threads in (128, 256, 512):
+    for lines in (0, 8, 16, 32):
         for per_sm in (0, 1, 2):
-            if batch.set_config(threads, per_sm) != 0:
+            if batch.set_config(lines, per_sm) != 0:
                 continue
             batch.run()
             st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -129,8 +130,8 @@ def tune_batch(batch, reps: int = 5, verbose: bool = False) -> tuple[int, int, f
             torch.cuda.synchronize()
             ms = st.elapsed_time(en) / reps
             if verbose:
-                print(f"  threads={threads} ctas/SM={per_sm or 'max'}: {ms:.3f} ms")
+                print(f"  lines={lines or 'auto'} ctas/SM={per_sm or 'max'}: {ms:.3f} ms")
             if best is None or ms < best[2]:
-                best = (threads, per_sm, ms)
+                best = (lines, per_sm, ms)
     batch.set_config(best[0], best[1])
     return best
