@@ -19,7 +19,9 @@ the host-buffer C-ABI call pado_apply_host, copies included), roofline of the
 line kernels (CUDA events, algorithmic bytes / kernel time, against the
 measured HBM copy bandwidth), cpu_baseline (the oracle -- the C restatement of
 the reference -- on the host cores), clocks sampled during the timed region,
-and the number of library kernel launches in the timed region.
+the number of library kernel launches in the timed region, and "extensions":
+the batched launch against the per-field loop on 96 uneven fields, and the
+adjoint against the forward operators on 256^3 (see extensions()).
 """
 from __future__ import annotations
 
@@ -180,6 +182,72 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def extensions() -> dict:
+    """The two extensions' own comparisons, each timed with CUDA events after
+    warm-up (inputs larger than L2):
+
+    * batched: 96 FP64 fields with dimensions drawn (seeded) from {32, ..., 384},
+      total <= 4 GiB, each cd06 or cd10, periodic or bounded, along a random
+      axis; one persistent launch replayed from a CUDA graph (tiles autotuned)
+      against the per-field loop of launches;
+    * adjoint: L = 0.5 ||D_x^cd10 u + D_z^cd06,bounded u - g||^2 on 256^3: the
+      two forward operators against their two adjoints (the backward pass).
+    """
+    import torch
+
+    import padeops_b200 as pb
+    from padeops_b200.batch import Batch
+    from padeops_b200.tune import tune_batch
+
+    def ev_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    rng = np.random.default_rng(4)
+    dims = (32, 48, 64, 96, 128, 192, 256, 384)
+    while True:
+        shapes = [tuple(int(v) for v in rng.choice(dims, 3)) for _ in range(96)]
+        if sum(a * b * c for a, b, c in shapes) * 8 <= 4 * 2 ** 30:
+            break
+    items, pts = [], 0
+    gen = torch.Generator(device="cuda").manual_seed(4)
+    for sh in shapes:
+        scheme, periodic, axis = int(rng.integers(2)), bool(rng.integers(2)), int(rng.integers(1, 4))
+        n = sh[3 - axis]
+        op = (pb.cd06 if scheme == 0 else pb.cd10)()
+        assert op.init(n, 2 * np.pi / n if periodic else 1.0 / (n - 1), periodic, 0, 0) == 0
+        fb = torch.randn(sh, dtype=torch.float64, device="cuda", generator=gen)
+        items.append((op, 1, axis, fb, torch.empty_like(fb), 0, 0))
+        pts += fb.numel()
+    batch = Batch(items)
+    lines, per_sm, _ = tune_batch(batch, reps=3)
+    loop_ms = ev_ms(batch.run_loop)
+    graph_ms = ev_ms(batch.run_graph)
+    batched = {"fields": len(items), "points": pts, "graph_ms": round(graph_ms, 3), "loop_ms": round(loop_ms, 3),
+               "speedup_vs_loop": round(loop_ms / graph_ms, 3), "graph_gpts": round(pts / graph_ms / 1e6, 1),
+               "tuned": {"lines": lines, "ctas_per_sm": per_sm}, "data": "seeded normal fields (timing only)"}
+    batch.destroy()
+    del items
+
+    n = 256
+    u = torch.randn(n ** 3, dtype=torch.float64, device="cuda", generator=gen)
+    o1, o2 = torch.empty_like(u), torch.empty_like(u)
+    dx_op, dz_op = pb.cd10(), pb.cd06()
+    assert dx_op.init(n, 2 * np.pi / n, True, 0, 0) == 0 and dz_op.init(n, 1.0 / (n - 1), False, 0, 0) == 0
+    fwd_ms = ev_ms(lambda: (dx_op.apply(1, 1, u, o1, n, n), dz_op.apply(1, 3, u, o2, n, n)))
+    adj_ms = ev_ms(lambda: (dx_op.apply(1, 1, u, o1, n, n, adjoint=True), dz_op.apply(1, 3, u, o2, n, n, adjoint=True)))
+    adjoint = {"workload": "D_x^cd10 (periodic) + D_z^cd06 (bounded) on 256^3", "fwd_ms": round(fwd_ms, 4),
+               "adjoint_ms": round(adj_ms, 4), "adjoint_over_forward": round(adj_ms / fwd_ms, 3)}
+    return {"batched": batched, "adjoint": adjoint}
+
+
 def run_gpu(args) -> None:
     import torch
 
@@ -273,6 +341,11 @@ def run_gpu(args) -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(f_host, os.cpu_count() or 1)
+    ext = None
+    if rank == 0 and world == 1 and not args.no_ext:
+        del f, df
+        torch.cuda.empty_cache()
+        ext = extensions()
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
@@ -286,7 +359,8 @@ def run_gpu(args) -> None:
                              "frac": round(achieved / peak, 4), "traffic": profiled_traffic(),
                              "kernel": "pado::stream_kernel (the 9 launches of a step, averaged)",
                              "peak_source": peak_kind},
-                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches}
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches,
+                "extensions": ext}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -327,6 +401,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pado", choices=["pado", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-ext", action="store_true", help="skip the batched / adjoint comparisons")
     ap.add_argument("--op", default=None, help="profiling: run only scheme:kind:axis (e.g. cf90:0:3)")
     ap.add_argument("--shape", default="512,128,512", help="profiling: field shape n3,n2,n1")
     ap.add_argument("--bounded", action="store_true", help="profiling: bounded instead of periodic lines")

@@ -204,11 +204,15 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     // candidates in order of preference (measured on 512^3: 16 lines and one
     // stage, two CTAs per SM, is fastest for every operator); the first that
     // fits two CTAs per SM wins, else the one with the most resident warps
-    int best_warps = 0, bestL = 0, best_stages = 0, best_ctas = 0;
+    int best_warps = 0, bestL = 0, best_stages = 0, best_ctas = 0, best_slots = 0;
+    unsigned char best_perm[KMAXSLOT] = {0};
     const int cand[6][2] = {{16, 1}, {32, 1}, {8, 1}, {16, 2}, {32, 2}, {8, 2}};
     for (const auto &c : cand) {
         const int L = c[0], stages = c[1];
-        if (L * S > 384) continue;  // the kernel is built for 384 threads, two CTAs per SM
+        // slots grouped by code path, padded to whole warps
+        unsigned char perm[KMAXSLOT];
+        const int nslots = warp_slots(dt.host, L, perm, KMAXSLOT);
+        if (L * nslots > 384) continue;  // the kernel is built for 384 threads, two CTAs per SM
         if (!xl && L == 32) continue;  // strided-line kernels exist for 8 and 16 lines per tile
         if (op->stream_lines && L != op->stream_lines) continue;
         if (op->stream_stages && stages != op->stream_stages) continue;
@@ -218,24 +222,20 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
         const size_t bytes = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows, resp_rows(kp0));
         if (bytes > 227 * 1024) continue;
         int ctas = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, fn, L * S, bytes) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, fn, L * nslots, bytes) != cudaSuccess) {
             (void)cudaGetLastError();
             continue;
         }
         if (ctas < 1) continue;
-        const int warps = ctas * ((L * S + 31) / 32);
-        if (ctas >= 2) {
+        const int warps = ctas * ((L * nslots + 31) / 32);
+        if (ctas >= 2 || warps > best_warps) {
             best_warps = warps;
             bestL = L;
             best_stages = stages;
             best_ctas = ctas;
-            break;
-        }
-        if (warps > best_warps) {
-            best_warps = warps;
-            bestL = L;
-            best_stages = stages;
-            best_ctas = ctas;
+            best_slots = nslots;
+            std::memcpy(best_perm, perm, sizeof(perm));
+            if (ctas >= 2) break;
         }
     }
     if (!best_warps) return false;
@@ -244,6 +244,8 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     std::memset(sp, 0, sizeof(*sp));
     sp->kp = kp0;
     sp->kp.L = L;
+    sp->kp.nslots = best_slots;
+    std::memcpy(sp->kp.sperm, best_perm, sizeof(best_perm));
     sp->kp.P = xl ? n + 2 : kp0.P;  // x: rows 16-byte aligned for the bulk copies
     sp->axis = axis;
     sp->stages = stages;
@@ -278,7 +280,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return false;
     }
-    *threads = L * S;
+    *threads = L * best_slots;
     *smem = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows, resp_rows(kp0));
     *ctas_per_sm = best_ctas;
     return true;
@@ -345,6 +347,7 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
         kp.xtab = dt.xtab_exact;
         set_chain(kp, dt.host.chain_exact);
         for (int i = 0; i < 32; ++i) kp.sperm[i] = (unsigned char)i;
+        kp.nslots = kp.S;
     }
     *kpo = kp;
     *trivial = false;

@@ -70,11 +70,22 @@ int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d,
     auto bytes = [&](int L_) {
         return batch_smem_doubles(L_, kp.S, kp.n, xl, kp.xd, erows, krows, resp_rows(kp)) * sizeof(double);
     };
-    int L = lines ? lines : std::min(64, (BATCH_THREADS / kp.S) & ~7);
-    if (L < 8 || L * kp.S > BATCH_THREADS) return PADO_E_SIZE;
-    while (L > 8 && bytes(L) > BATCH_SMEM_CAP) L -= 8;
-    if (bytes(L) > BATCH_SMEM_CAP) return PADO_E_SIZE;
+    // the most lines (64, 32, 16, 8) whose slots (grouped by code path,
+    // padded to whole warps) fit the CTA and whose tile fits the cap
+    int L = 0, nslots = 0;
+    unsigned char perm[KMAXSLOT];
+    for (int cand : {64, 32, 16, 8}) {
+        if (lines && cand != lines) continue;
+        const int ns = warp_slots(dt.host, cand, perm, KMAXSLOT);
+        if (cand * ns > BATCH_THREADS || bytes(cand) > BATCH_SMEM_CAP) continue;
+        L = cand;
+        nslots = ns;
+        break;
+    }
+    if (!L) return PADO_E_SIZE;
     kp.L = L;
+    kp.nslots = nslots;
+    std::memcpy(kp.sperm, perm, sizeof(perm));
     std::memset(d, 0, sizeof(*d));
     d->kp = kp;
     d->etab = dt.etab;

@@ -123,7 +123,7 @@ __device__ __noinline__ void batch_tile(const BatchItemDev &it, double *smem, lo
     __syncthreads();
 
     const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
-    const bool active = slot < S;
+    const bool active = s >= 0;
     const long long rs = XL ? 1 : (long long)L;
     double *line = sm.tile + (XL ? (size_t)l * P : (size_t)l);
     typename RL::Halo h;

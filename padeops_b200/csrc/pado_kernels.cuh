@@ -35,6 +35,8 @@
 namespace pado {
 
 constexpr int KMAXM = 64;  // longest segment (MAXM of pado_tables.h)
+constexpr int KMAXSLOT = 48;  // thread slots per line (segments plus warp padding)
+constexpr unsigned char SLOT_IDLE = 0xff;
 constexpr int KCT_NF = 4;  // border-sum weights per segment (CT_NF of pado_tables.h)
 
 // Parameters of one launch (passed by value).
@@ -63,7 +65,8 @@ struct KParams {
     unsigned spk_mask;     // bit s: ... and adds its rows' cyclic spike terms (per-row table)
     double kc[8];          // alpha, c1, c2, gamma, d1, d2, delta
     double pu[KMAXM], pv[KMAXM], ps[KMAXM], pt[KMAXM];  // unit responses, rows 0..m-1
-    unsigned char sperm[32];  // thread slot -> segment (per-row-table segments first)
+    unsigned char sperm[KMAXSLOT];  // thread slot -> segment, SLOT_IDLE for an idle slot
+    int nslots;                     // slots per line (S, or more when warps are padded)
     unsigned short sstart[33];  // segment s = rows [sstart[s], sstart[s+1])
     unsigned char wf[32], wb[32];    // coupling window of each segment (forward, backward)
     unsigned short xof[32], xob[32]; // first xtab block of each segment's forward / backward list
@@ -78,8 +81,11 @@ PADO_HD PADO_INLINE const double *resp_row(const KParams &kp, const double *rtab
 }
 PADO_HD PADO_INLINE int resp_rows(const KParams &kp) { return kp.ie + (kp.nb - kp.je); }
 
-// Segment of thread slot `slot` (= tid / L); slots >= S are idle.
-PADO_HD PADO_INLINE int slot_segment(const KParams &kp, int slot) { return slot < kp.S ? kp.sperm[slot] : slot; }
+// Segment of thread slot `slot` (= tid / L), or -1 for an idle slot.
+PADO_HD PADO_INLINE int slot_segment(const KParams &kp, int slot)
+{
+    return (slot < kp.nslots && kp.sperm[slot] != SLOT_IDLE) ? (int)kp.sperm[slot] : -1;
+}
 
 PADO_HD PADO_INLINE int seg_start(const KParams &kp, int s) { return kp.sstart[s]; }
 PADO_HD PADO_INLINE int seg_len(const KParams &kp, int s) { return kp.sstart[s + 1] - kp.sstart[s]; }
@@ -788,7 +794,7 @@ PADO_HD PADO_INLINE void tile_phase(int phase, const KParams &kp, const Smem &sm
 {
     using K = LineKernel<RK, PER, ADJ, M, IN>;
     const int l = tid % kp.L, slot = tid / kp.L, s = slot_segment(kp, slot);
-    const bool active = slot < kp.S;
+    const bool active = s >= 0;
     switch (phase) {
     case PH_LOAD: tile_load(kp, sm, q0, tid, nthreads); break;
     case PH_FWD:
@@ -934,7 +940,7 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
     const Smem sm = carve(smem_raw, kp.L, kp.P, kp.S, kp.xd);
     const int tid = threadIdx.x, nthreads = blockDim.x;
     const int l = tid % kp.L, slot = tid / kp.L, s = slot_segment(kp, slot);
-    const bool active = slot < kp.S;
+    const bool active = s >= 0;
     const long long ntiles = (kp.nlines + kp.L - 1) / kp.L;
     Regs<M> R;
     long long t = blockIdx.x;

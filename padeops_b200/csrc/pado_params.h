@@ -35,7 +35,8 @@ inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn
     std::memcpy(kp.pv, in.pv, sizeof(kp.pv));
     std::memcpy(kp.ps, in.ps, sizeof(kp.ps));
     std::memcpy(kp.pt, in.pt, sizeof(kp.pt));
-    std::memcpy(kp.sperm, ot.sperm, sizeof(kp.sperm));
+    std::memcpy(kp.sperm, ot.sperm, sizeof(ot.sperm));
+    kp.nslots = kp.S;
     kp.ie = ot.ie;
     kp.je = ot.nbord > 0 ? ot.je : ot.nb;
     set_chain(kp, ot.chain);

@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
 
     const int tid = threadIdx.x, nthreads = blockDim.x;
     const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
-    const bool active = slot < S;
+    const bool active = s >= 0;
     const long long G = gridDim.x;
     const long long t_first = blockIdx.x;
     const int stages = sp.stages;
@@ -406,7 +406,7 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
             if (ph == 5 && !adj_tile) continue;
             for (int tid = 0; tid < nthreads; ++tid) {
                 const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
-                if (slot >= S) continue;
+                if (s < 0) continue;
                 double *line = sm.tile + l * ls;
                 const LineIO io = stream_line_io(sp, sm, l, t);
                 switch (ph) {

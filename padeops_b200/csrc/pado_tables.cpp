@@ -747,6 +747,41 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     return ot;
 }
 
+int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots)
+{
+    const int S = ot.lay.S;
+    auto cls = [&](int s) {
+        if (!((ot.interior.mask >> s) & 1u)) return 0;
+        const bool spk = (ot.interior.spk_mask >> s) & 1u;
+        const int a = ot.lay.start(s), len = ot.lay.len(s);
+        const bool resp = ot.nbord > 0 && (a < ot.ie || a + len > ot.je);
+        return spk ? (resp ? 1 : 2) : (resp ? 3 : 4);
+    };
+    const int spw = L >= 32 ? 1 : 32 / L;
+    int k = 0;
+    for (int c = 0; c <= 4; ++c) {
+        int cnt = 0;
+        for (int s = 0; s < S; ++s)
+            if (cls(s) == c) {
+                if (k >= max_slots) break;
+                sperm[k++] = (unsigned char)s;
+                ++cnt;
+            }
+        while (cnt % spw != 0 && k < max_slots) {
+            sperm[k++] = 0xff;
+            ++cnt;
+        }
+    }
+    int used = 0;
+    for (int i = 0; i < k; ++i) used += sperm[i] != 0xff;
+    if (used != S) {
+        // does not fit: the unpadded order
+        std::memcpy(sperm, ot.sperm, (size_t)S);
+        return S;
+    }
+    return k;
+}
+
 std::vector<double> stencil_matrix(const RhsCoef &rc, int n, int bc1, int bcn)
 {
     std::vector<double> B((size_t)n * n, 0.0);

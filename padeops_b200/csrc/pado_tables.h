@@ -135,6 +135,16 @@ struct OpTables {
 };
 OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, int bc1, int bcn, int m, bool adjoint);
 
+// Thread-slot order for kernels whose threads are (line tid % L, slot
+// tid / L): segments grouped by the code path they take -- per-row table;
+// constant-coefficient with cyclic spike sums and border responses; with
+// spike sums only; with border responses only; plain constant-coefficient --
+// each group padded with idle slots (0xff) to whole warps (32 / L slots per
+// warp), so that no warp runs two paths one after the other.  Returns the
+// slot count, or the unpadded order's S when the padded one needs more than
+// max_slots.
+int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots);
+
 // Transposed stencil of a bounded line: B^T rows for the first and last
 // ZB columns.  Dense (n x n) when n <= DENSE_BT_MAX.
 constexpr int BT_ZONE = 8, BT_WIN = 12, DENSE_BT_MAX = 32;

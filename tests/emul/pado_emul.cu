@@ -68,6 +68,7 @@ extern "C" int emul_apply(int scheme, int kind, int n, double dx, int periodic, 
         kp.int_mask = 0u;
         kp.spk_mask = 0u;
         for (int i = 0; i < 32; ++i) kp.sperm[i] = (unsigned char)i;
+        kp.nslots = kp.S;
     }
     const int nthreads = lines * lay.S + extra_threads;
     switch (ot.rc.rk) {
@@ -139,7 +140,8 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
         sp.ntiles = (long long)sp.xblocks * nb;
         sp.pstride = axis == 2 ? na * (long long)n : na;
     }
-    const int nthreads = lines * lay.S;
+    kp.nslots = warp_slots(ot, lines, kp.sperm, KMAXSLOT);
+    const int nthreads = lines * kp.nslots;
     const bool per = periodic != 0;
     switch (ot.rc.rk) {
     case RHS_CD06_D1:
