@@ -246,6 +246,7 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     sp->kp.L = L;
     sp->kp.nslots = best_slots;
     std::memcpy(sp->kp.sperm, best_perm, sizeof(best_perm));
+    sp->kp.border_slot = first_idle_slot(best_perm, best_slots);
     sp->kp.P = xl ? n + 2 : kp0.P;  // x: rows 16-byte aligned for the bulk copies
     sp->axis = axis;
     sp->stages = stages;

@@ -86,6 +86,7 @@ int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d,
     kp.L = L;
     kp.nslots = nslots;
     std::memcpy(kp.sperm, perm, sizeof(perm));
+    kp.border_slot = first_idle_slot(perm, nslots);
     std::memset(d, 0, sizeof(*d));
     d->kp = kp;
     d->etab = dt.etab;

@@ -132,6 +132,7 @@ __device__ __noinline__ void batch_tile(const BatchItemDev &it, double *smem, lo
     if (active) RL::template fwd<true>(kp, sm, line, rs, l, s, h);
     __syncthreads();
     if (active) RL::template bwd<true>(kp, sm, line, rs, l, s);
+    else if (PER && slot == kp.border_slot) RL::border_only(kp, sm, l);
     __syncthreads();
     if (XL) {
         if (active) RL::template fin<true>(kp, sm, line, rs, l, s, line, 1, true);

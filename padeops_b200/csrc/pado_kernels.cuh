@@ -67,6 +67,8 @@ struct KParams {
     double pu[KMAXM], pv[KMAXM], ps[KMAXM], pt[KMAXM];  // unit responses, rows 0..m-1
     unsigned char sperm[KMAXSLOT];  // thread slot -> segment, SLOT_IDLE for an idle slot
     int nslots;                     // slots per line (S, or more when warps are padded)
+    int border_slot;                // idle slot whose threads solve a cyclic line's border
+                                    // unknowns (-1: segment 0's threads do)
     unsigned short sstart[33];  // segment s = rows [sstart[s], sstart[s+1])
     unsigned char wf[32], wb[32];    // coupling window of each segment (forward, backward)
     unsigned short xof[32], xob[32]; // first xtab block of each segment's forward / backward list

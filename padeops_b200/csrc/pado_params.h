@@ -37,6 +37,7 @@ inline void fill_params(KParams &kp, const OpTables &ot, int n, int bc1, int bcn
     std::memcpy(kp.pt, in.pt, sizeof(kp.pt));
     std::memcpy(kp.sperm, ot.sperm, sizeof(ot.sperm));
     kp.nslots = kp.S;
+    kp.border_slot = -1;
     kp.ie = ot.ie;
     kp.je = ot.nbord > 0 ? ot.je : ot.nb;
     set_chain(kp, ot.chain);

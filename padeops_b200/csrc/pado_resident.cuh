@@ -317,6 +317,17 @@ struct ResidentLine {
         Q2 = a2 + b2;
     }
 
+    // the border unknowns of line l, for fin (the backward sweeps run with
+    // E = 0); by an idle slot's threads where the warps are padded, else by
+    // segment 0's threads
+    static PADO_HD PADO_INLINE void border_only(const KParams &kp, const Smem &sm, int l)
+    {
+        double E1, E2;
+        border(kp, sm, l, E1, E2);
+        sm.eb[(size_t)l * 4 + 0] = E1;
+        sm.eb[(size_t)l * 4 + 1] = E2;
+    }
+
     // ---- bwd: local backward sweep, x written over z ------------------------
     template <bool STAGED>
     static PADO_HD PADO_INLINE void bwd(const KParams &kp, const Smem &sm, double *line, long long rs, int l, int s)
@@ -328,13 +339,7 @@ struct ResidentLine {
         double P1, P2;
         incoming_fwd(kp, sm, l, s, P1, P2);
         double x1 = 0.0, x2 = 0.0;
-        if (CYC && s == 0) {
-            // the border unknowns, for fin (the sweep itself runs with E = 0)
-            double E1, E2;
-            border(kp, sm, l, E1, E2);
-            sm.eb[(size_t)l * 4 + 0] = E1;
-            sm.eb[(size_t)l * 4 + 1] = E2;
-        }
+        if (CYC && s == 0 && kp.border_slot < 0) border_only(kp, sm, l);
         if (fast(kp, s)) {
             bwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, P1, P2, 0.0, 0.0, x1, x2);
         } else {
@@ -366,12 +371,18 @@ struct ResidentLine {
     static PADO_HD PADO_INLINE void fin_fast(const KParams &kp, const Smem &sm, const double *p, long long rs, double *q,
                                              long long os, int a, double Q1, double Q2, double E1, double E2)
     {
+        // response rows: t < tl (first region, rows a + t) and t >= tr (last
+        // region, packed after the first one), each at a fixed offset from a
+        // per-segment base
+        const int tl = RSP ? kp.ie - a : 0, tr = RSP ? kp.je - a : M;
+        const double *rl = RSP ? sm.rtab + (long long)a * 2 : nullptr;
+        const double *rr_ = RSP ? sm.rtab + (long long)(kp.ie - kp.je + a) * 2 : nullptr;
 #pragma unroll
         for (int t = 0; t < M; ++t) {
             double x = p[(long long)t * rs] + Q1 * kp.ps[t];
             if (ORDER2) x += Q2 * kp.pt[t];
-            if (RSP && (a + t < kp.ie || a + t >= kp.je)) {
-                const double *rr = resp_row(kp, sm.rtab, a + t);
+            if (RSP && (t < tl || t >= tr)) {
+                const double *rr = (t < tl ? rl : rr_) + 2 * t;
                 x += E1 * rr[0];
                 if (ORDER2) x += E2 * rr[1];
             }

@@ -318,6 +318,7 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
         if (active) RL::template fwd<true>(kp, sm, line, rs, l, s, h);
         __syncthreads();
         if (active) RL::template bwd<true>(kp, sm, line, rs, l, s);
+        else if (PER && slot == kp.border_slot) RL::border_only(kp, sm, l);
         __syncthreads();
         // adjoint x lines: fbar over z in the tile, then the bulk stores, when
         // the end columns of B^T fit the summary buffers (free after fin)
@@ -406,7 +407,10 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
             if (ph == 5 && !adj_tile) continue;
             for (int tid = 0; tid < nthreads; ++tid) {
                 const int l = tid % L, slot = tid / L, s = slot_segment(kp, slot);
-                if (s < 0) continue;
+                if (s < 0) {
+                    if (PER && ph == 2 && slot == kp.border_slot) RL::border_only(kp, sm, l);
+                    continue;
+                }
                 double *line = sm.tile + l * ls;
                 const LineIO io = stream_line_io(sp, sm, l, t);
                 switch (ph) {

@@ -144,6 +144,13 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
 // slot count, or the unpadded order's S when the padded one needs more than
 // max_slots.
 int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots);
+// First idle slot of a slot order (-1: none).
+inline int first_idle_slot(const unsigned char *sperm, int nslots)
+{
+    for (int k = 0; k < nslots; ++k)
+        if (sperm[k] == 0xff) return k;
+    return -1;
+}
 
 // Transposed stencil of a bounded line: B^T rows for the first and last
 // ZB columns.  Dense (n x n) when n <= DENSE_BT_MAX.

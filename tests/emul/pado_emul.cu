@@ -141,6 +141,7 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
         sp.pstride = axis == 2 ? na * (long long)n : na;
     }
     kp.nslots = warp_slots(ot, lines, kp.sperm, KMAXSLOT);
+    kp.border_slot = first_idle_slot(kp.sperm, kp.nslots);
     const int nthreads = lines * kp.nslots;
     const bool per = periodic != 0;
     switch (ot.rc.rk) {
