@@ -211,7 +211,8 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
         const int L = c[0], stages = c[1];
         // slots grouped by code path, padded to whole warps
         unsigned char perm[KMAXSLOT];
-        const int nslots = warp_slots(dt.host, L, perm, KMAXSLOT);
+        int nslots = warp_slots(dt.host, L, perm, KMAXSLOT, true);
+        if (L * nslots > 384) nslots = warp_slots(dt.host, L, perm, KMAXSLOT, false);
         if (L * nslots > 384) continue;  // the kernel is built for 384 threads, two CTAs per SM
         if (!xl && L == 32) continue;  // strided-line kernels exist for 8 and 16 lines per tile
         if (op->stream_lines && L != op->stream_lines) continue;

@@ -76,7 +76,8 @@ int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d,
     unsigned char perm[KMAXSLOT];
     for (int cand : {64, 32, 16, 8}) {
         if (lines && cand != lines) continue;
-        const int ns = warp_slots(dt.host, cand, perm, KMAXSLOT);
+        int ns = warp_slots(dt.host, cand, perm, KMAXSLOT, true);
+        if (cand * ns > BATCH_THREADS) ns = warp_slots(dt.host, cand, perm, KMAXSLOT, false);
         if (cand * ns > BATCH_THREADS || bytes(cand) > BATCH_SMEM_CAP) continue;
         L = cand;
         nslots = ns;

@@ -199,7 +199,7 @@ struct ResidentLine {
             if (ADJ) {
                 r = p[(long long)t * rs];
             } else {
-                r = rhs_interior(RK, PER, cst, w);
+                r = rhs_interior_fma(RK, PER, cst, w);
                 if (first && t < CR) r = pick4(h.cv, t);
                 if (last && a + t >= n - CR) r = pick4(h.cl, a + t - (n - CR));
             }

@@ -747,7 +747,7 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     return ot;
 }
 
-int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots)
+int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots, bool border_warp)
 {
     const int S = ot.lay.S;
     auto cls = [&](int s) {
@@ -759,6 +759,10 @@ int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots)
     };
     const int spw = L >= 32 ? 1 : 32 / L;
     int k = 0;
+    if (border_warp && ot.nbord > 0) {
+        // a warp of idle slots first: its first slot is the first idle one
+        for (int j = 0; j < spw && k < max_slots; ++j) sperm[k++] = 0xff;
+    }
     for (int c = 0; c <= 4; ++c) {
         int cnt = 0;
         for (int s = 0; s < S; ++s)

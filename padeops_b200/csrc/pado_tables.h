@@ -140,10 +140,11 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
 // constant-coefficient with cyclic spike sums and border responses; with
 // spike sums only; with border responses only; plain constant-coefficient --
 // each group padded with idle slots (0xff) to whole warps (32 / L slots per
-// warp), so that no warp runs two paths one after the other.  Returns the
-// slot count, or the unpadded order's S when the padded one needs more than
-// max_slots.
-int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots);
+// warp), so that no warp runs two paths one after the other.  border_warp:
+// one warp of idle slots first (cyclic lines), whose first slot -- the
+// first idle one -- solves the border unknowns while the others sweep.  Returns the slot count, or the
+// unpadded order's S when the padded one needs more than max_slots.
+int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots, bool border_warp = false);
 // First idle slot of a slot order (-1: none).
 inline int first_idle_slot(const unsigned char *sperm, int nslots)
 {

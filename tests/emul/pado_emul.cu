@@ -140,7 +140,7 @@ extern "C" int emul_stream(int scheme, int kind, int n, double dx, int periodic,
         sp.ntiles = (long long)sp.xblocks * nb;
         sp.pstride = axis == 2 ? na * (long long)n : na;
     }
-    kp.nslots = warp_slots(ot, lines, kp.sperm, KMAXSLOT);
+    kp.nslots = warp_slots(ot, lines, kp.sperm, KMAXSLOT, true);
     kp.border_slot = first_idle_slot(kp.sperm, kp.nslots);
     const int nthreads = lines * kp.nslots;
     const bool per = periodic != 0;
