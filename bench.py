@@ -43,6 +43,8 @@ N = 512
 OPS = [("cd10", 1), ("cd10", 2), ("cf90", 0)]  # (scheme, kind)
 METRIC = "Gpts/s cd06/cd10 dd1-3 @512^3 FP64 (%HBM peak); batched, fwd+adjoint vs plain"
 BYTES_PER_PT = 16
+CONFIG = {"workload": "cd10 d1 + cd10 d2 + cf90, periodic, x/y/z on 512^3 FP64 (9 operator applications per step)",
+          "n": N, "operators_per_step": 9, "l2": "inputs larger than L2 (1 GiB field)"}
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -172,8 +174,7 @@ def run_reference(args) -> None:
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gpts/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 9 * N ** 3 / (v * 1e9) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "cd10 d1 + cd10 d2 + cf90, periodic, x/y/z on 512^3 FP64", "n": N,
-                       "operators_per_step": 9},
+            "config": dict(CONFIG),
             "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": threads, "kind": "port",
                              "sample": "the full 9-operator step on the 512^3 field per timed step "
                                        "(oracle = C restatement of the reference; the Fortran reference "
@@ -253,17 +254,11 @@ def run_gpu(args) -> None:
 
     import padeops_b200 as pb
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from padeops_b200 import dist as pdist
+
+    rank, world, local = pdist.world()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = pdist.init("nccl")
 
     dx = 2 * np.pi / N
     f_host = make_field(7 + rank)
@@ -302,13 +297,8 @@ def run_gpu(args) -> None:
         stop.record(stream)
         torch.cuda.synchronize()
     launches = pb.launch_count() - launches0
-    ms = start.elapsed_time(stop)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    pts = 9 * N ** 3 * args.steps * world
-    value = pts / (ms / 1e3) / 1e9
+    ms = pdist.max_over_ranks(start.elapsed_time(stop), dist, "cuda")
+    value = pdist.weak_scaling_rate(9 * N ** 3 * args.steps, world, ms / 1e3) / 1e9
     kern_ms = [a.elapsed_time(b) for row in ev for a, b in row]
     per_op = {}
     for i, (op, kind, axis) in enumerate(plan):
@@ -351,10 +341,7 @@ def run_gpu(args) -> None:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "cd10 d1 + cd10 d2 + cf90, periodic, x/y/z on 512^3 FP64 "
-                                       "(9 operator applications per step)",
-                           "n": N, "operators_per_step": 9, "l2": "inputs larger than L2 (1 GiB field)",
-                           "per_operator_gbs": per_op},
+                "config": dict(CONFIG, per_operator_gbs=per_op),
                 "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(achieved / peak, 4), "traffic": profiled_traffic(),
                              "kernel": "pado::stream_kernel (the 9 launches of a step, averaged)",
