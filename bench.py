@@ -361,6 +361,9 @@ def run_single_op(args) -> None:
 
     import padeops_b200 as pb
 
+    if args.op == "batch":
+        run_batch_profile(args)
+        return
     scheme, kind, axis = args.op.split(":")
     kind, axis = int(kind), int(axis)
     n3, n2, n1 = (int(v) for v in args.shape.split(","))
@@ -376,9 +379,38 @@ def run_single_op(args) -> None:
     print(json.dumps({"op": args.op, "shape": [n3, n2, n1], "periodic": periodic,
                       "plan": op.launch_plan(kind, axis, f, df, na, nb)}), flush=True)
     for _ in range(args.repeat):
-        op.apply(kind, axis, f, df, na, nb)
+        op.apply(kind, axis, f, df, na, nb, adjoint=args.adjoint)
     torch.cuda.synchronize()
     assert op.device_status() == 0
+
+
+def run_batch_profile(args) -> None:
+    """The batched launch on a seeded uneven batch of about 1 GiB of inputs
+    (cd06 / cd10 first derivatives, dimensions from {32, ..., 256}, periodic or
+    bounded, random axis): the small case of the batch kernel's ncu summary."""
+    import torch
+
+    import padeops_b200 as pb
+    from padeops_b200.batch import Batch
+
+    rng = np.random.default_rng(4)
+    dims = (32, 48, 64, 96, 128, 192, 256)
+    items, total = [], 0
+    gen = torch.Generator(device="cuda").manual_seed(4)
+    while total < 2 ** 30:
+        sh = tuple(int(v) for v in rng.choice(dims, 3))
+        scheme, periodic, axis = int(rng.integers(2)), bool(rng.integers(2)), int(rng.integers(1, 4))
+        n = sh[3 - axis]
+        op = (pb.cd06 if scheme == 0 else pb.cd10)()
+        assert op.init(n, 0.1, periodic, 0, 0) == 0
+        f = torch.randn(sh, dtype=torch.float64, device="cuda", generator=gen)
+        items.append((op, 1, axis, f, torch.empty_like(f), 0, 0))
+        total += f.numel() * 8
+    b = Batch(items)
+    print(json.dumps({"op": "batch", "fields": len(items), "input_bytes": total, "info": b.info()}), flush=True)
+    for _ in range(args.repeat):
+        b.run()
+    torch.cuda.synchronize()
 
 
 def main() -> None:
@@ -389,10 +421,12 @@ def main() -> None:
     ap.add_argument("--impl", default="pado", choices=["pado", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-ext", action="store_true", help="skip the batched / adjoint comparisons")
-    ap.add_argument("--op", default=None, help="profiling: run only scheme:kind:axis (e.g. cf90:0:3)")
+    ap.add_argument("--op", default=None,
+                    help="profiling: run only scheme:kind:axis (e.g. cf90:0:3), or 'batch' (an uneven 1 GiB batch)")
     ap.add_argument("--shape", default="512,128,512", help="profiling: field shape n3,n2,n1")
     ap.add_argument("--bounded", action="store_true", help="profiling: bounded instead of periodic lines")
     ap.add_argument("--repeat", type=int, default=3, help="profiling: applications of the operator")
+    ap.add_argument("--adjoint", action="store_true", help="profiling: the adjoint operator")
     args = ap.parse_args()
     if args.op:
         run_single_op(args)
