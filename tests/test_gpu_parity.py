@@ -275,3 +275,45 @@ def test_apply_host_pipeline(torch_cuda, axis):
             out2 = np.full(shape, np.nan)
             op.apply_host(kind, axis, f, out2, na, nb)
             assert rel_err(out2, ref) <= TOL, (shape, scheme, kind, "pageable")
+
+
+def test_bounded_config_full_size(torch_cuda):
+    """The bounded workload at its full size, 1024 x 512 x 256 (x, y periodic; z
+    bounded, dz = 1/255): f = P3(z) + 0.1 sin(kx x + ky y), seeded.  Checked
+    through properties that hold at any size: the bounded cd06 and cd10 first
+    derivatives along z reproduce P3'(z) (their closures are exact for cubics),
+    and the periodic cd10 first derivatives along x and y equal the modified
+    wavenumber times the sine's derivative (<= 1e-11 relative)."""
+    from tests.recipes import mod_wavenumber
+
+    torch = torch_cuda
+    n1, n2, n3 = 1024, 512, 256
+    rng = np.random.default_rng(3)
+    c = rng.uniform(-1, 1, 4)
+    kx, ky = (int(v) for v in rng.integers(1, 33, 2))
+    dx, dy, dz = 2 * np.pi / n1, 2 * np.pi / n2, 1.0 / (n3 - 1)
+    x = torch.arange(n1, dtype=torch.float64, device="cuda") * dx
+    y = torch.arange(n2, dtype=torch.float64, device="cuda") * dy
+    z = torch.arange(n3, dtype=torch.float64, device="cuda") * dz
+    phase = kx * x[None, None, :] + ky * y[None, :, None]
+    f = (c[0] + c[1] * z + c[2] * z ** 2 + c[3] * z ** 3)[:, None, None] + 0.1 * torch.sin(phase)
+    f = f.contiguous()
+    df = torch.empty_like(f)
+    dp3 = (c[1] + 2 * c[2] * z + 3 * c[3] * z ** 2)[:, None, None].expand(n3, n2, n1)
+
+    def rel(a, b):
+        return float((a - b).abs().max() / b.abs().max())
+
+    for scheme in (oracle.CD06, oracle.CD10):
+        op = _make(scheme, n3, dz, False)
+        op.apply(oracle.D1, 3, f, df, n1, n2, 0, 0)
+        torch.cuda.synchronize()
+        assert rel(df, dp3) <= 1e-11, (scheme, rel(df, dp3))
+    cos = 0.1 * torch.cos(phase).expand(n3, n2, n1)
+    for axis, n, d, k in ((1, n1, dx, kx), (2, n2, dy, ky)):
+        op = _make(oracle.CD10, n, d, True)
+        na, nb = na_nb((n3, n2, n1), axis)
+        op.apply(oracle.D1, axis, f, df, na, nb, 0, 0)
+        torch.cuda.synchronize()
+        ref = mod_wavenumber(oracle.CD10, oracle.D1, k, d) * cos
+        assert rel(df, ref) <= 1e-11, (axis, rel(df, ref))
