@@ -113,6 +113,17 @@ int pado_apply(pado_op_t op, int kind, int axis, const double *f, double *df, lo
 int pado_apply_adjoint(pado_op_t op, int kind, int axis, const double *g, double *fbar, long na, long nb, int bc1,
                        int bcn, void *stream);
 
+/* cf90%filter3 for a complex field -- filter3_CMPLX, cf90.F90:1230-1251.
+ * f and df are complex (na,nb,n) arrays: (re, im) pairs of doubles, as the
+ * Fortran complex(rkind) type stores them.  As in the reference, the
+ * right-hand side takes the closures (bc1, bcn) and the solve always uses the
+ * bc (0, 0) system (penta_nn); a Fortran caller passes bc1 = bcn = 0 when it
+ * omits bcn_ (the reference reads bc1_ only when bcn_ is present).  A
+ * periodic object has no penta_nn system: PADO_E_UNSUPPORTED (the reference
+ * indexes an unallocated array there).  n == 1 copies f. */
+int pado_filter3_complex(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn,
+                         void *stream);
+
 /* Host-buffer variant of pado_apply for callers whose fields live in host
  * memory (the reference's own calling convention): copies f to the device,
  * applies the operator and copies df back, pipelined in chunks, and returns

@@ -68,6 +68,9 @@ def library(fast: bool = False) -> ctypes.CDLL:
     lib.oracle_apply.restype = ctypes.c_int
     lib.oracle_table.argtypes = [P, ctypes.c_int, P]
     lib.oracle_table.restype = ctypes.c_int
+    lib.oracle_filter3_complex.argtypes = [P, P, P, ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int]
+    lib.oracle_filter3_complex.restype = ctypes.c_int
     _libs[name] = lib
     return lib
 
@@ -107,6 +110,19 @@ class OracleOp:
         rc = self.lib.oracle_apply(self._h, kind, axis, f.ctypes.data, df.ctypes.data, na, nb, bc1, bcn, nthreads)
         if rc != 0:
             raise RuntimeError(f"oracle_apply returned {rc}")
+        return df
+
+    def filter3_complex(self, f: np.ndarray, na: int, nb: int, bc1: int = 0, bcn: int = 0,
+                        nthreads: int = 1) -> np.ndarray:
+        """cf90%filter3 of a complex (na,nb,n) field (filter3_CMPLX, cf90.F90:1230):
+        right-hand side with closures (bc1, bcn), solve with the bc (0,0) system."""
+        f = np.ascontiguousarray(f, dtype=np.complex128)
+        if f.size != self.n * na * nb:
+            raise ValueError(f"field has {f.size} elements, expected {self.n * na * nb}")
+        df = np.empty_like(f)
+        rc = self.lib.oracle_filter3_complex(self._h, f.ctypes.data, df.ctypes.data, na, nb, bc1, bcn, nthreads)
+        if rc != 0:
+            raise RuntimeError(f"oracle_filter3_complex returned {rc}")
         return df
 
     def table(self, which: int, ncol: int) -> np.ndarray:

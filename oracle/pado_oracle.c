@@ -1010,4 +1010,37 @@ int oracle_apply(const oracle_op *op, int kind, int axis, const double *f, doubl
     return 0;
 }
 
+/* cf90.F90:1230-1251  filter3_CMPLX.  A complex (na,nb,n) field stores (re, im)
+ * pairs, so to the stencil and the solve -- which act on each part alone -- it
+ * is the real (2*na,nb,n) field.  The right-hand side takes the closures
+ * (bc1, bcn) (ComputeZRHS_CMPLX, CF90_files/ComputeZRHS_common.F90); the solve
+ * always uses penta_nn (SolveZPenta_CMPLX, CF90_files/SolveZPenta_common.F90).
+ * Returns 0; -3 for a periodic object (it has no penta_nn: the reference reads
+ * an unallocated array); 324 for a bc outside {0, 1, -1} (the reference does
+ * not check and leaves those rows unset). */
+int oracle_filter3_complex(const oracle_op *op, const double *f, double *df, long na, long nb, int bc1, int bcn,
+                           int nthreads)
+{
+    const int n = op->n;
+    const long nl = 2 * na * nb;
+    if (op->scheme != SCHEME_CF90) return -2;
+    if (n == 1) {
+        for (long q = 0; q < nl; ++q) df[q] = f[q];
+        return 0;
+    }
+    if (op->periodic) return -3;
+    if ((bc1 != 0 && bc1 != 1 && bc1 != -1) || (bcn != 0 && bcn != 1 && bcn != -1)) return 324;
+    if (nthreads < 1) nthreads = 1;
+    const long chunks = nthreads > 1 ? 4L * nthreads : 1;
+    const long cl = (nl + chunks - 1) / chunks;
+#pragma omp parallel for schedule(static) num_threads(nthreads) if (nthreads > 1)
+    for (long c = 0; c < chunks; ++c) {
+        const long l0 = c * cl, l1 = l0 + cl < nl ? l0 + cl : nl;
+        if (l1 <= l0) continue;
+        rhs_block(op, KIND_FILTER, f + l0, df + l0, (int)(l1 - l0), nl, bc1, bcn);
+        solve_penta(op->penta1[pidx(0, 0)], n, df + l0, (int)(l1 - l0), nl);
+    }
+    return 0;
+}
+
 int oracle_n(const oracle_op *op) { return op->n; }

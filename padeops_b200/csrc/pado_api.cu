@@ -311,7 +311,8 @@ int launch_stream(pado_op_s *op, const StreamParams &sp, bool adj, int threads, 
 }  // namespace
 
 int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
-                         int bcn, bool adjoint, int lines, bool no_fast, KParams *kpo, bool *trivial)
+                         int bcn, bool adjoint, int lines, bool no_fast, KParams *kpo, bool *trivial, int solve_bc1,
+                         int solve_bcn)
 {
     *trivial = true;
     if (!op) return PADO_E_NULL;
@@ -327,7 +328,8 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
     if (f < df + total && df < f + total) return PADO_E_ALIAS;
     if (n == 1) return PADO_OK;
     const bool bounded_bc = !op->periodic && op->scheme != CD06;
-    auto it = op->tables.find(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, adjoint ? 1 : 0));
+    const int sb1 = solve_bc1 == SAME_BC ? bc1 : solve_bc1, sbn = solve_bcn == SAME_BC ? bcn : solve_bcn;
+    auto it = op->tables.find(TabKey(kind, bounded_bc ? sb1 : 0, bounded_bc ? sbn : 0, adjoint ? 1 : 0));
     if (it == op->tables.end()) return PADO_E_STATE;
     const DevTables &dt = it->second;
 
@@ -359,11 +361,12 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
 namespace {
 
 int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1, int bcn,
-           cudaStream_t st, bool adjoint)
+           cudaStream_t st, bool adjoint, int solve_bc1 = SAME_BC, int solve_bcn = SAME_BC)
 {
     KParams kp;
     bool trivial = true;
-    int rc = prepare_launch(op, kind, axis, f, df, na, nb, bc1, bcn, adjoint, op ? op->lines : 0, false, &kp, &trivial);
+    int rc = prepare_launch(op, kind, axis, f, df, na, nb, bc1, bcn, adjoint, op ? op->lines : 0, false, &kp, &trivial,
+                            solve_bc1, solve_bcn);
     if (rc != PADO_OK) return rc;
     if (trivial) {
         const long long total = (long long)op->n * na * nb;
@@ -375,7 +378,8 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
     }
     if (op->variant == 0 || op->variant == 4) {
         const bool bounded_bc = !op->periodic && op->scheme != CD06;
-        const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, adjoint ? 1 : 0));
+        const int sb1 = solve_bc1 == SAME_BC ? bc1 : solve_bc1, sbn = solve_bcn == SAME_BC ? bcn : solve_bcn;
+        const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? sb1 : 0, bounded_bc ? sbn : 0, adjoint ? 1 : 0));
         StreamParams sp;
         int sthreads = 0, sctas = 0;
         size_t ssmem = 0;
@@ -500,6 +504,19 @@ int pado_apply_adjoint(pado_op_t op, int kind, int axis, const double *g, double
                        int bcn, void *stream)
 {
     return launch(op, kind, axis, g, fbar, na, nb, bc1, bcn, (cudaStream_t)stream, true);
+}
+
+int pado_filter3_complex(pado_op_t op, const double *f, double *df, long na, long nb, int bc1, int bcn,
+                         void *stream)
+{
+    if (!op) return PADO_E_NULL;
+    if (op->scheme != CF90) return PADO_E_UNSUPPORTED;
+    if (na < 0 || nb < 0) return PADO_E_ARG;
+    // a periodic object has no penta_nn system (cf90.F90:1249 would read an unallocated array)
+    if (op->periodic && op->n != 1) return PADO_E_UNSUPPORTED;
+    // interleaved (re, im): the real (2 na, nb, n) field, each part filtered alone; the
+    // right-hand side takes the closures (bc1, bcn), the solve always the bc (0, 0) system
+    return launch(op, FILTER, 3, f, df, 2 * na, nb, bc1, bcn, (cudaStream_t)stream, false, 0, 0);
 }
 
 #define PADO_NAMED(name, kind, axis)                                                                        \

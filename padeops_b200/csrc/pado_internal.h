@@ -82,7 +82,11 @@ StreamFn pick_stream_rk3(bool per, int m, bool xl, int lines, bool adj);
 
 // no_fast: every segment on the per-row table (for kernels built for a
 // segment length other than the handle's).
+// solve_bc1/solve_bcn: the closures whose system is solved, when they differ
+// from the right-hand side's (bc1, bcn); SAME_BC: the same.
+constexpr int SAME_BC = 99;
 int prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
-                   int bcn, bool adjoint, int lines, bool no_fast, KParams *kp, bool *trivial);
+                   int bcn, bool adjoint, int lines, bool no_fast, KParams *kp, bool *trivial, int solve_bc1 = SAME_BC,
+                   int solve_bcn = SAME_BC);
 
 }  // namespace pado

@@ -244,7 +244,20 @@ class cf90(_Scheme):  # noqa: N801
         return self.apply(L.FILTER, 2, f, df, na, nb, bc1_, bcn_)
 
     def filter3(self, f, df, na, nb, bc1_=None, bcn_=None):
-        """cf90%filter3 (cf90.F90:1160, real variant)."""
+        """cf90%filter3 (cf90.F90:1160); a complex128 f and df take the complex
+        variant (filter3_CMPLX, cf90.F90:1230-1251): right-hand side with the
+        closures (bc1_, bcn_) -- bc1_ only when bcn_ is given, as in the
+        reference -- and the solve with the bc (0,0) system."""
+        if f.dtype == torch.complex128:
+            if df.dtype != torch.complex128 or not (f.is_cuda and df.is_cuda and f.is_contiguous() and df.is_contiguous()):
+                raise ValueError("complex filter3: f and df must be contiguous complex128 CUDA tensors")
+            bc1, bcn = (0, 0) if bcn_ is None else (int(bc1_ or 0), int(bcn_))
+            fr, dfr = torch.view_as_real(f), torch.view_as_real(df)
+            with torch.cuda.device(f.device):
+                st = L.lib().pado_filter3_complex(self.handle, fr.data_ptr(), dfr.data_ptr(), int(na), int(nb), bc1,
+                                                  bcn, _stream_ptr(fr))
+            check(st, "cf90.filter3 (complex)")
+            return df
         return self.apply(L.FILTER, 3, f, df, na, nb, bc1_, bcn_)
 
 

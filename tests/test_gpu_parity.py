@@ -317,3 +317,39 @@ def test_bounded_config_full_size(torch_cuda):
         torch.cuda.synchronize()
         ref = mod_wavenumber(oracle.CD10, oracle.D1, k, d) * cos
         assert rel(df, ref) <= 1e-11, (axis, rel(df, ref))
+
+
+def test_complex_z_filter(torch_cuda):
+    """cf90 filter3 on complex fields (filter3_CMPLX) through pado_filter3_complex:
+    every closure pair on the right-hand side, the bc (0,0) solve, against the
+    oracle (<= 1e-12); a periodic object is refused; n == 1 copies."""
+    import padeops_b200 as pb
+    from padeops_b200._lib import PadoError
+
+    torch = torch_cuda
+    rng = np.random.default_rng(77)
+    for n, na, nb in ((10, 3, 2), (33, 8, 5), (256, 20, 6)):
+        f = rng.standard_normal((n, nb, na)) + 1j * rng.standard_normal((n, nb, na))
+        o = oracle.OracleOp(oracle.CF90, n, 1.0, False)
+        op = pb.cf90()
+        assert op.init(n, False) == 0
+        ft = torch.from_numpy(f).cuda()
+        for bc1, bcn in BCS:
+            out = torch.full_like(ft, complex(float("nan"), float("nan")))
+            op.filter3(ft, out, na, nb, bc1, bcn)
+            torch.cuda.synchronize()
+            ref = o.filter3_complex(f, na, nb, bc1, bcn).reshape(f.shape)
+            got = out.cpu().numpy()
+            assert np.abs(got - ref).max() / np.abs(ref).max() <= TOL, (n, bc1, bcn)
+    per = pb.cf90()
+    assert per.init(64, True) == 0
+    ft = torch.zeros((64, 2, 2), dtype=torch.complex128, device="cuda")
+    with pytest.raises(PadoError):
+        per.filter3(ft, torch.empty_like(ft), 2, 2)
+    one = pb.cf90()
+    assert one.init(1, True) == 0
+    ft = torch.from_numpy(rng.standard_normal((1, 2, 3)) + 1j).cuda()
+    out = torch.empty_like(ft)
+    one.filter3(ft, out, 3, 2)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ft)

@@ -157,3 +157,25 @@ def test_golden_fixtures():
         na, nb = na_nb(f.shape, c["axis"])
         got = o.apply(c["kind"], c["axis"], f, na, nb, c["bc1"], c["bcn"]).reshape(f.shape)
         assert np.array_equal(got, data[f"df{i}"]), c
+
+
+def test_complex_z_filter():
+    """filter3_CMPLX (cf90.F90:1230-1251): the real and imaginary parts are
+    filtered alone, the right-hand side with the closures (bc1, bcn) and the
+    solve with the bc (0,0) system -- so for bc (0,0) it equals the real
+    filter3 of each part, and for other closures it equals A_00^{-1} B_bc."""
+    rng = np.random.default_rng(8)
+    n, na, nb = 40, 3, 2
+    o = oracle.OracleOp(oracle.CF90, n, 1.0, False)
+    f = rng.standard_normal((n, nb, na)) + 1j * rng.standard_normal((n, nb, na))
+    for bc1, bcn in itertools.product([0, 1, -1], [0, 1, -1]):
+        got = o.filter3_complex(f, na, nb, bc1, bcn).reshape(f.shape)
+        D = np.linalg.solve(dense.lhs(oracle.CF90, oracle.FILTER, n, False, 0, 0),
+                            dense.rhs(oracle.CF90, oracle.FILTER, n, 1.0, False, bc1, bcn))
+        ref = dense.apply_axis(D, f.real, 3) + 1j * dense.apply_axis(D, f.imag, 3)
+        assert np.abs(got - ref).max() / np.abs(ref).max() <= 1e-12, (bc1, bcn)
+        if (bc1, bcn) == (0, 0):
+            re = o.apply(oracle.FILTER, 3, np.ascontiguousarray(f.real), na, nb).reshape(f.shape)
+            assert np.array_equal(got.real, re)
+    with pytest.raises(RuntimeError, match="-3"):
+        oracle.OracleOp(oracle.CF90, n, 1.0, True).filter3_complex(f, na, nb)
