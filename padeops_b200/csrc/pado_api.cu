@@ -45,8 +45,8 @@ bool kind_supported(int scheme, int kind)
 namespace {
 
 // host-buffer pipeline: about this many bytes per chunk, at most this many chunks
-constexpr size_t HOST_CHUNK_BYTES = size_t(64) << 20;
-constexpr size_t HOST_MAX_CHUNKS = 32;
+constexpr size_t HOST_CHUNK_BYTES = size_t(16) << 20;
+constexpr size_t HOST_MAX_CHUNKS = 128;
 
 int max_threads_for_m(int m) { return m >= 64 ? 256 : 512; }
 
