@@ -228,12 +228,13 @@ def extensions() -> dict:
         items.append((op, 1, axis, fb, torch.empty_like(fb), 0, 0))
         pts += fb.numel()
     batch = Batch(items)
-    lines, per_sm, _ = tune_batch(batch, reps=3)
+    lines, per_sm, branches, _ = tune_batch(batch, reps=3)
     loop_ms = ev_ms(batch.run_loop)
     graph_ms = ev_ms(batch.run_graph)
     batched = {"fields": len(items), "points": pts, "graph_ms": round(graph_ms, 3), "loop_ms": round(loop_ms, 3),
                "speedup_vs_loop": round(loop_ms / graph_ms, 3), "graph_gpts": round(pts / graph_ms / 1e6, 1),
-               "tuned": {"lines": lines, "ctas_per_sm": per_sm}, "data": "seeded normal fields (timing only)"}
+               "tuned": {"lines": lines, "ctas_per_sm": per_sm, "graph_branches": branches},
+               "data": "seeded normal fields (timing only)"}
     batch.destroy()
     del items
 

@@ -188,8 +188,16 @@ int pado_batch_create(pado_batch_t *batch, const pado_batch_item *items, int nit
 int pado_batch_run(pado_batch_t batch, void *stream);
 /* Enqueue the batch as one launch per item (the per-field loop it replaces). */
 int pado_batch_run_loop(pado_batch_t batch, void *stream);
-/* Capture pado_batch_run into a CUDA graph once and replay it on `stream`. */
+/* Capture the batch into a CUDA graph once and replay it on `stream`.  The
+ * graph holds the persistent launch of pado_batch_run, or, after
+ * pado_batch_set_graph_branches(batch, k) with k > 0, one streaming-kernel
+ * launch per item dealt to k concurrent branches (items of different sizes
+ * then share the GPU instead of running one after another). */
 int pado_batch_run_graph(pado_batch_t batch, void *stream);
+/* What pado_batch_run_graph captures: 0 = the persistent launch (default),
+ * 1..16 = per-item launches on that many concurrent graph branches.  Drops
+ * any captured graph.  Used by the autotuner. */
+int pado_batch_set_graph_branches(pado_batch_t batch, int branches);
 /* Launch shape of the persistent kernel: lines per tile (8/16/32/64; 0 =
  * enough lines to keep every thread of the CTA busy, 384 / segments per line,
  * within the shared-memory cap) and a cap on resident CTAs per SM (0 = as

@@ -68,6 +68,7 @@ SIGNATURES = {
                              ctypes.POINTER(ctypes.c_longlong)]),
     "pado_batch_destroy": (None, [_P]),
     "pado_batch_run_static": (_I, [_P, _I, _P]),
+    "pado_batch_set_graph_branches": (_I, [_P, _I]),
     "pado_filter3_complex": (_I, [_P, _P, _P, _L, _L, _I, _I, _P]),
     "pado_strerror": (ctypes.c_char_p, [_I]),
     "pado_launch_count": (ctypes.c_longlong, []),

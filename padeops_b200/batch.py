@@ -50,6 +50,11 @@ class Batch:
         """One launch per item (the per-field loop the batch replaces)."""
         check(L.lib().pado_batch_run_loop(self._h, self._stream()), "pado_batch_run_loop")
 
+    def set_graph_branches(self, branches: int) -> int:
+        """What run_graph captures: 0 = the persistent launch, k > 0 = one
+        streaming-kernel launch per item on k concurrent graph branches."""
+        return L.lib().pado_batch_set_graph_branches(self._h, branches)
+
     def set_config(self, lines: int = 0, ctas_per_sm: int = 0) -> int:
         """Lines per tile (8, 16, 32, 64; 0 = automatic) and a cap on CTAs per SM (0 = none)."""
         return L.lib().pado_batch_set_config(self._h, lines, ctas_per_sm)

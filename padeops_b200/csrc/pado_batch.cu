@@ -25,6 +25,11 @@ struct pado_batch_s {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t capture_stream = nullptr;
+    // graph contents: 0 = the persistent launch; k > 0 = one streaming-kernel
+    // launch per item, the items dealt round-robin to k concurrent branches
+    int branches = 0;
+    std::vector<cudaStream_t> branch_streams;
+    std::vector<cudaEvent_t> branch_events;  // [0]: fork, [1 + k]: branch k done
 };
 
 namespace {
@@ -195,9 +200,56 @@ int enqueue_persistent(pado_batch_s *b, cudaStream_t st)
     return e == cudaSuccess ? PADO_OK : cuda_fail(e);
 }
 
+// Per-item launches on b->branches concurrent branches of stream `st` (fork
+// and join by events, so that a stream capture records them as parallel
+// branches of one graph).
+int enqueue_branches(pado_batch_s *b, cudaStream_t st)
+{
+    const int k = b->branches;
+    while ((int)b->branch_streams.size() < k) {
+        cudaStream_t s = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(e);
+        b->branch_streams.push_back(s);
+    }
+    while ((int)b->branch_events.size() < k + 1) {
+        cudaEvent_t ev = nullptr;
+        cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e);
+        b->branch_events.push_back(ev);
+    }
+    cudaError_t e = cudaEventRecord(b->branch_events[0], st);
+    for (int j = 0; j < k && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(b->branch_streams[j], b->branch_events[0], 0);
+    if (e != cudaSuccess) return cuda_fail(e);
+    int rc = PADO_OK;
+    for (size_t i = 0; i < b->items.size() && rc == PADO_OK; ++i) {
+        const pado_batch_item &it = b->items[i];
+        const long long na = it.axis == 1 ? it.n2 : it.n1;
+        const long long nb = it.axis == 3 ? it.n2 : it.n3;
+        rc = pado_apply(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn,
+                        b->branch_streams[i % k]);
+    }
+    // join every branch, also after an error, so that a capture can end
+    for (int j = 0; j < k && e == cudaSuccess; ++j) {
+        e = cudaEventRecord(b->branch_events[1 + j], b->branch_streams[j]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->branch_events[1 + j], 0);
+    }
+    if (rc != PADO_OK) return rc;
+    return e == cudaSuccess ? PADO_OK : cuda_fail(e);
+}
+
 }  // namespace
 
 extern "C" {
+
+int pado_batch_set_graph_branches(pado_batch_t b, int branches)
+{
+    if (!b) return PADO_E_NULL;
+    if (branches < 0 || branches > 16) return PADO_E_ARG;
+    b->branches = branches;
+    drop_graph(b);
+    return PADO_OK;
+}
 
 int pado_batch_create(pado_batch_t *out, const pado_batch_item *items, int nitems)
 {
@@ -258,9 +310,17 @@ int pado_batch_run_graph(pado_batch_t b, void *stream)
             cudaError_t e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
             if (e != cudaSuccess) return cuda_fail(e);
         }
+        if (b->branches > 0) {
+            // one uncaptured pass first: the per-item launches set their kernels'
+            // attributes on first use, which a capture must not record
+            int rc0 = pado_batch_run_loop(b, b->capture_stream);
+            if (rc0 != PADO_OK) return rc0;
+            cudaError_t e0 = cudaStreamSynchronize(b->capture_stream);
+            if (e0 != cudaSuccess) return cuda_fail(e0);
+        }
         cudaError_t e = cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_fail(e);
-        int rc = enqueue_persistent(b, b->capture_stream);
+        int rc = b->branches > 0 ? enqueue_branches(b, b->capture_stream) : enqueue_persistent(b, b->capture_stream);
         cudaGraph_t g = nullptr;
         e = cudaStreamEndCapture(b->capture_stream, &g);
         if (rc != PADO_OK) {
@@ -283,6 +343,8 @@ void pado_batch_destroy(pado_batch_t b)
 {
     if (!b) return;
     drop_graph(b);
+    for (cudaStream_t s : b->branch_streams) cudaStreamDestroy(s);
+    for (cudaEvent_t ev : b->branch_events) cudaEventDestroy(ev);
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_tile0s) cudaFree(b->d_tile0s);

@@ -113,25 +113,42 @@ def tune_op(op, kind: int, axis: int, shape: tuple[int, int, int], reps: int = 5
     return best
 
 
-def tune_batch(batch, reps: int = 5, verbose: bool = False) -> tuple[int, int, float]:
-    """Pick the persistent kernel's (lines per tile, CTAs per SM) for a batch.
-    Returns (lines, ctas_per_sm, ms); 0 means automatic / no cap."""
+def _time(fn, reps: int) -> float:
+    fn()
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.record()
+    for _ in range(reps):
+        fn()
+    en.record()
+    torch.cuda.synchronize()
+    return st.elapsed_time(en) / reps
+
+
+def tune_batch(batch, reps: int = 5, verbose: bool = False, branches=(0, 2, 4, 8)) -> tuple[int, int, int, float]:
+    """Autotune a batch: the persistent kernel's (lines per tile, CTAs per SM),
+    then what its CUDA graph holds -- the persistent launch (0) or one
+    streaming-kernel launch per item on k concurrent branches -- by timing the
+    graph replay.  Returns (lines, ctas_per_sm, branches, ms); 0 means
+    automatic / no cap / the persistent launch."""
     best = None
     for lines in (0, 8, 16, 32):
         for per_sm in (0, 1, 2):
             if batch.set_config(lines, per_sm) != 0:
                 continue
-            batch.run()
-            st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            st.record()
-            for _ in range(reps):
-                batch.run()
-            en.record()
-            torch.cuda.synchronize()
-            ms = st.elapsed_time(en) / reps
+            ms = _time(batch.run, reps)
             if verbose:
-                print(f"  lines={lines or 'auto'} ctas/SM={per_sm or 'max'}: {ms:.3f} ms")
+                print(f"  persistent lines={lines or 'auto'} ctas/SM={per_sm or 'max'}: {ms:.3f} ms")
             if best is None or ms < best[2]:
                 best = (lines, per_sm, ms)
     batch.set_config(best[0], best[1])
-    return best
+    choice = None
+    for k in branches:
+        if batch.set_graph_branches(k) != 0:
+            continue
+        ms = _time(batch.run_graph, reps)
+        if verbose:
+            print(f"  graph {'persistent launch' if k == 0 else f'{k} branches of per-item launches'}: {ms:.3f} ms")
+        if choice is None or ms < choice[1]:
+            choice = (k, ms)
+    batch.set_graph_branches(choice[0])
+    return best[0], best[1], choice[0], choice[1]

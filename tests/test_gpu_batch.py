@@ -95,12 +95,34 @@ def test_batch_autotuner_keeps_results():
 
     items, host = _items(torch, 16, seed=9)
     b = Batch(items)
-    lines, per_sm, ms = tune_batch(b, reps=2)
-    assert lines in (0, 8, 16, 32) and per_sm in (0, 1, 2) and ms > 0
+    lines, per_sm, branches, ms = tune_batch(b, reps=2)
+    assert lines in (0, 8, 16, 32) and per_sm in (0, 1, 2) and branches in (0, 2, 4, 8) and ms > 0
     for it in items:
         it[4].fill_(float("nan"))
     b.run()
     _check(torch, items, host)
+    for it in items:
+        it[4].fill_(float("nan"))
+    b.run_graph()
+    _check(torch, items, host)
+    b.destroy()
+
+
+@pytest.mark.parametrize("branches", [1, 4])
+def test_batch_graph_of_branches(branches):
+    """The graph of per-item streaming-kernel launches on concurrent branches."""
+    import torch
+
+    from padeops_b200.batch import Batch
+
+    items, host = _items(torch, 30, seed=13)
+    b = Batch(items)
+    assert b.set_graph_branches(branches) == 0
+    for _ in range(2):
+        for it in items:
+            it[4].fill_(float("nan"))
+        b.run_graph()
+        _check(torch, items, host)
     b.destroy()
 
 
