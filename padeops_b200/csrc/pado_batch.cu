@@ -202,7 +202,7 @@ int enqueue_persistent(pado_batch_s *b, cudaStream_t st)
 
 // Per-item launches on b->branches concurrent branches of stream `st` (fork
 // and join by events, so that a stream capture records them as parallel
-// branches of one graph).
+// branches of one graph), dealt largest first to the least-loaded branch.
 int enqueue_branches(pado_batch_s *b, cudaStream_t st)
 {
     const int k = b->branches;
@@ -221,13 +221,21 @@ int enqueue_branches(pado_batch_s *b, cudaStream_t st)
     cudaError_t e = cudaEventRecord(b->branch_events[0], st);
     for (int j = 0; j < k && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(b->branch_streams[j], b->branch_events[0], 0);
     if (e != cudaSuccess) return cuda_fail(e);
+    // largest items first, each to the branch with the least work so far
+    std::vector<size_t> order(b->items.size());
+    std::iota(order.begin(), order.end(), size_t(0));
+    auto points = [&](size_t i) { return (double)b->items[i].n1 * b->items[i].n2 * b->items[i].n3; };
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return points(x) > points(y); });
+    std::vector<double> load(k, 0.0);
     int rc = PADO_OK;
-    for (size_t i = 0; i < b->items.size() && rc == PADO_OK; ++i) {
+    for (size_t i : order) {
         const pado_batch_item &it = b->items[i];
         const long long na = it.axis == 1 ? it.n2 : it.n1;
         const long long nb = it.axis == 3 ? it.n2 : it.n3;
-        rc = pado_apply(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn,
-                        b->branch_streams[i % k]);
+        const int j = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[j] += points(i);
+        rc = pado_apply(it.op, it.kind, it.axis, it.f, it.df, (long)na, (long)nb, it.bc1, it.bcn, b->branch_streams[j]);
+        if (rc != PADO_OK) break;
     }
     // join every branch, also after an error, so that a capture can end
     for (int j = 0; j < k && e == cudaSuccess; ++j) {
