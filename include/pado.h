@@ -22,7 +22,9 @@
  *     cd06 ignores them (its closures are fixed at init), as do periodic
  *     operators.
  *   - Handles are immutable after init and may be used concurrently from
- *     several host threads and streams.
+ *     several host threads and streams -- except through the tuning setters
+ *     (pado_set_tiling, pado_set_kernel_variant, pado_set_stream_tiling),
+ *     which change the handle and must not overlap other calls on it.
  *
  * Differences from the reference, by design:
  *   - f and df are DEVICE pointers and the work is enqueued on `stream`

@@ -41,6 +41,28 @@ def max_over_ranks(value: float, dist, device: str | torch.device = "cpu") -> fl
     return float(t.item())
 
 
+def partition_fields(costs, world_size: int) -> list[list[int]]:
+    """Assigns fields to ranks by LPT bin packing (largest first, each to the
+    least-loaded rank): the field-level data parallelism of a batch of uneven
+    fields.  costs[i] is field i's work (points x the scheme's relative cost);
+    returns, per rank, the field indices it runs (each rank then builds its own
+    batch of them -- no data moves between ranks)."""
+    import heapq
+
+    if world_size < 1:
+        raise ValueError("world_size must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    heap = [(0.0, r) for r in range(world_size)]
+    parts: list[list[int]] = [[] for _ in range(world_size)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        parts[r].append(i)
+        heapq.heappush(heap, (load + float(costs[i]), r))
+    for p in parts:
+        p.sort()
+    return parts
+
+
 def weak_scaling_rate(points_per_rank: float, world_size: int, max_seconds: float) -> float:
     """Whole-job throughput (points per second) when every rank processed
     points_per_rank points and the slowest took max_seconds."""

@@ -54,3 +54,21 @@ def test_single_process_needs_no_group(monkeypatch):
     monkeypatch.delenv("WORLD_SIZE", raising=False)
     assert pdist.init("gloo") is None
     assert pdist.max_over_ranks(3.5, None) == 3.5
+
+
+def test_partition_fields_lpt():
+    """Uneven fields split over ranks by LPT: every field once, loads within the
+    largest field of each other (the LPT bound), deterministic."""
+    import numpy as np
+
+    from padeops_b200 import dist as pdist
+
+    rng = np.random.default_rng(96)
+    dims = (32, 48, 64, 96, 128, 192, 256, 384)
+    costs = [float(np.prod(rng.choice(dims, 3))) * (1.0 if rng.integers(2) else 1.4) for _ in range(96)]
+    for world in (1, 2, 4, 8):
+        parts = pdist.partition_fields(costs, world)
+        assert sorted(i for p in parts for i in p) == list(range(96))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(costs)
+        assert parts == pdist.partition_fields(costs, world)
