@@ -353,3 +353,52 @@ def test_complex_z_filter(torch_cuda):
     one.filter3(ft, out, 3, 2)
     torch.cuda.synchronize()
     assert torch.equal(out, ft)
+
+
+def test_field_operators(torch_cuda):
+    """gradient / curl / divergence / filter3D (operators.F90 counterparts) against
+    the same compositions of oracle operators: cd10 periodic x and y, cd06 bounded
+    z (closures from init), cf90 periodic x, y and bounded z; numtimes = 2."""
+    import padeops_b200 as pb
+    from padeops_b200 import field_ops
+
+    torch = torch_cuda
+    n1, n2, n3 = 24, 20, 18
+    shape = (n3, n2, n1)
+    rng = np.random.default_rng(11)
+    u, v, w = (rng.standard_normal(shape) for _ in range(3))
+    dx, dy, dz = 2 * np.pi / n1, 2 * np.pi / n2, 1.0 / (n3 - 1)
+    der = pb.Derivatives()
+    der.init(n1, n2, n3, dx, dy, dz, True, True, False, "cd10", "cd10", "cd06")
+    fil = pb.Filters()
+    fil.init(n1, n2, n3, "cf90", "cf90", "cf90", True, True, False)
+
+    def od(axis, f, bc=(0, 0)):
+        scheme, n, d, per = {1: (oracle.CD10, n1, dx, True), 2: (oracle.CD10, n2, dy, True),
+                             3: (oracle.CD06, n3, dz, False)}[axis]
+        return _oracle_apply(scheme, oracle.D1, axis, f, d, per, *bc)
+
+    def ofil(axis, f, bc=(0, 0)):
+        per = axis != 3
+        return _oracle_apply(oracle.CF90, oracle.FILTER, axis, f, 1.0, per, *bc)
+
+    T = lambda a: torch.from_numpy(a).cuda()
+    gx, gy, gz = (torch.empty(shape, dtype=torch.float64, device="cuda") for _ in range(3))
+    field_ops.gradient(der, T(u), gx, gy, gz)
+    for got, axis in ((gx, 1), (gy, 2), (gz, 3)):
+        assert rel_err(got.cpu().numpy(), od(axis, u)) <= TOL
+    cu = torch.empty((3,) + shape, dtype=torch.float64, device="cuda")
+    field_ops.curl(der, T(u), T(v), T(w), cu)
+    ref = [od(2, w) - od(3, v), od(3, u) - od(1, w), od(1, v) - od(2, u)]
+    for k in range(3):
+        assert rel_err(cu[k].cpu().numpy(), ref[k]) <= TOL, k
+    div = torch.empty(shape, dtype=torch.float64, device="cuda")
+    field_ops.divergence(der, T(u), T(v), T(w), div)
+    assert rel_err(div.cpu().numpy(), od(1, u) + od(2, v) + od(3, w)) <= TOL
+    arr = T(u).clone()
+    field_ops.filter3d(fil, arr, numtimes=2, z_bc=(1, -1))
+    ref = u
+    for axis, bc in ((2, (0, 0)), (1, (0, 0)), (3, (1, -1))):
+        for _ in range(2):
+            ref = ofil(axis, ref, bc)
+    assert rel_err(arr.cpu().numpy(), ref) <= TOL
