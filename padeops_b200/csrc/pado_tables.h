@@ -84,7 +84,8 @@ Interior interior_info(const Sweep &sw, const Layout &lay, int m);
 //   Q_s = sum_{j>s} Psi(s,j) w_j,  Psi(s,j) = B_{s+1} ... B_{j-1}
 // (y_j, w_j: the local end / first values of segment j).  The products decay
 // like the sweep's homogeneous solutions; those below XFER_DROP are dropped,
-// which bounds the window W.
+// which bounds the window W (a dropped product moves the result by less than
+// 1e-17 of the coupled segment's end value, far below FP64 rounding).
 //   xtab: packed 2x2 blocks (4 doubles, row-major): Phi(s, s-d) for d =
 //         1..wf[s] from block xof[s], Psi(s, s+d) for d = 1..wb[s] from xob[s]
 //   ctab [S][CT_NF]: G1_s, G2_s with G_s = sum_{t>s} k_t Phi(t, s), k_t the
@@ -92,7 +93,7 @@ Interior interior_info(const Sweep &sw, const Layout &lay, int m);
 //                    sum_s (local sum_s + G_s . y_s)
 // Constant-coefficient segments take the responses of Interior.
 constexpr int CT_NF = 4;
-constexpr double XFER_DROP = 1e-20;
+constexpr double XFER_DROP = 1e-17;
 struct ChainTables {
     std::vector<double> ctab, xtab;
     int W = 0;  // largest window
