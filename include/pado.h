@@ -141,15 +141,19 @@ int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, doub
 int pado_set_tiling(pado_op_t op, int m, int lines);
 int pado_get_tiling(pado_op_t op, int *m, int *lines);
 /* Kernel organisation of the forward operator: 0 = automatic (the
- * streaming kernel where the field allows it, else 1; the default),
+ * streaming kernel where the field allows it; else 5 for x lines and cd06,
+ * 1 otherwise, as measured fastest; the default),
  * 1 = one CTA per tile of lines, 2 = persistent CTAs that prefetch the next
  * tile with cp.async while the current one is solved, 3 = persistent CTAs
  * that read lines straight into registers and warm L2 with the next tile
  * (strided axes; x lines use 2), 4 = the streaming kernel: persistent CTAs
  * fed by TMA tensor / bulk copies two tiles ahead (needs 16-byte aligned
  * fields, an even x extent for y/z lines and an even n for x lines;
- * PADO_E_UNSUPPORTED otherwise).  Adjoints follow the same choice (4 runs
- * the transposed sweep in the tile, then B^T); 2 and 3 mean 1 for adjoints.
+ * PADO_E_UNSUPPORTED otherwise), 5 = the streaming kernel's resident tiles
+ * fed by plain loads (any extent and alignment; segments of 16 or 32 rows,
+ * i.e. n <= 1024; PADO_E_UNSUPPORTED otherwise).  Adjoints follow the same
+ * choice (4 runs the transposed sweep in the tile, then B^T); 2, 3 and 5
+ * mean 1 for adjoints.
  * No counterpart in the reference (a B200 tuning knob). */
 int pado_set_kernel_variant(pado_op_t op, int variant);
 /* Tiling of the streaming kernel: lines per tile (8/16 for y/z lines,

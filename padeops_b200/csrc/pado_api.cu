@@ -50,6 +50,12 @@ constexpr size_t HOST_MAX_CHUNKS = 128;
 
 int max_threads_for_m(int m) { return m >= 64 ? 256 : 512; }
 
+// When the streaming kernel cannot run, the automatic choice takes the
+// resident tiles with plain loads (variant 5) where they beat the line kernel
+// (measured at 511^3): x lines, and the tridiagonal cd06 sweeps on any axis;
+// the line kernel elsewhere.
+bool resident_fallback(const pado_op_s *op, int axis) { return axis == 1 || op->scheme == CD06; }
+
 // Default tiling: segment length and lines per CTA for a line of length n.
 void default_tiling(int n, int *m, int *lines)
 {
@@ -387,6 +393,11 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
             return launch_stream(op, sp, adjoint, sthreads, ssmem, sctas, st);
         if (op->variant == 4) return PADO_E_UNSUPPORTED;
     }
+    if ((op->variant == 5 || (op->variant == 0 && resident_fallback(op, axis))) && !adjoint && solve_bc1 == SAME_BC) {
+        // the same resident tiles, with plain loads
+        rc = launch_resident_single(op, kind, axis, f, df, na, nb, bc1, bcn, st);
+        if (rc != PADO_E_UNSUPPORTED || op->variant == 5) return rc;
+    }
     // lines per CTA: the handle's choice, halved until the segments fit
     while (kp.L > 1 && kp.L * kp.S > max_threads_for_m(op->m)) kp.L /= 2;
     const int threads = kp.L * kp.S;
@@ -650,7 +661,7 @@ int pado_set_tiling(pado_op_t op, int m, int lines)
 int pado_set_kernel_variant(pado_op_t op, int variant)
 {
     if (!op) return PADO_E_NULL;
-    if (variant < 0 || variant > 4) return PADO_E_ARG;
+    if (variant < 0 || variant > 5) return PADO_E_ARG;
     op->variant = variant;
     return PADO_OK;
 }
@@ -682,6 +693,9 @@ int pado_launch_plan(pado_op_t op, int kind, int axis, const double *f, double *
             return PADO_OK;
         }
     }
+    if ((op->variant == 5 || (op->variant == 0 && resident_fallback(op, axis))) &&
+        launch_resident_single(op, kind, axis, f, df, na, nb, bc1, bcn, nullptr, info) == PADO_OK)
+        return PADO_OK;
     info[0] = op->variant == 0 ? 1 : op->variant;
     info[1] = kp.L;
     info[6] = kp.L * kp.S;

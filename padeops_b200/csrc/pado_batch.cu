@@ -108,6 +108,59 @@ int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d,
     return PADO_OK;
 }
 
+// The resident single-field kernel (single_kernel) for one apply; returns
+// PADO_E_UNSUPPORTED when the field does not fit its rules (segments of 16 or
+// 32 rows, the tile within the shared-memory cap), so that the caller can use
+// the line kernel instead.  info (not null): fill the launch plan the way
+// pado_launch_plan reports it and launch nothing.
+int launch_resident_single(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb,
+                           int bc1, int bcn, cudaStream_t st, int *info)
+{
+    pado_batch_item it{};
+    it.op = op;
+    it.kind = kind;
+    it.axis = axis;
+    it.bc1 = bc1;
+    it.bcn = bcn;
+    it.n1 = axis == 1 ? op->n : na;
+    it.n2 = axis == 1 ? na : (axis == 2 ? op->n : nb);
+    it.n3 = axis == 3 ? op->n : nb;
+    it.f = f;
+    it.df = df;
+    BatchItemDev d;
+    long long tiles = 0;
+    double cost = 0;
+    size_t smem = 0;
+    bool skip = false;
+    const int rc = batch_item_descriptor(it, 0, &d, &tiles, &cost, &smem, &skip);
+    if (rc == PADO_E_SIZE) return PADO_E_UNSUPPORTED;
+    if (rc != PADO_OK || skip) return rc;
+    d.tile0 = 0;
+    cudaError_t e = cudaFuncSetAttribute((const void *)single_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)BATCH_SMEM_CAP);
+    if (e != cudaSuccess) return cuda_fail(e);
+    int per_sm = 0, dev = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, single_kernel, BATCH_THREADS, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (per_sm < 1) return PADO_E_UNSUPPORTED;
+    if (info) {
+        info[0] = 5;
+        info[1] = d.kp.L;
+        info[2] = 1;
+        info[3] = per_sm;
+        info[6] = d.kp.L * d.kp.nslots;
+        info[7] = (int)smem;
+        return PADO_OK;
+    }
+    const long long grid = std::max<long long>(1, std::min<long long>(tiles, (long long)per_sm * sms));
+    single_kernel<<<(unsigned)grid, BATCH_THREADS, smem, st>>>(d);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? PADO_OK : cuda_fail(e);
+}
+
 }  // namespace pado
 
 namespace {

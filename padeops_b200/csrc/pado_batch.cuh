@@ -215,6 +215,37 @@ __global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) batch_kernel(co
         }
     }
 }
+
+// One field whose lines the streaming kernel's copy engine cannot move (an odd
+// extent, an unaligned pointer): the same resident tiles with plain loads,
+// the descriptor a kernel parameter, tiles strided over the grid.
+__global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) single_kernel(const __grid_constant__ BatchItemDev it)
+{
+    extern __shared__ double smem_raw[];
+    batch_stage(it, batch_carve(it, smem_raw));
+    const long long ntiles = (it.kp.nlines + it.kp.L - 1) / it.kp.L;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        __syncthreads();  // tables staged / the previous tile's buffer free
+        const long long q0 = t * it.kp.L;
+        switch (it.code) {
+#define PADO_CASE_M(rk, per, xl)                                                             \
+    case ((rk * 2 + per) * 2 + xl) * 2 + 0: batch_tile<rk, per, 16, xl>(it, smem_raw, q0); break; \
+    case ((rk * 2 + per) * 2 + xl) * 2 + 1: batch_tile<rk, per, 32, xl>(it, smem_raw, q0); break;
+#define PADO_CASE(rk)                  \
+    PADO_CASE_M(rk, false, false)      \
+    PADO_CASE_M(rk, false, true)       \
+    PADO_CASE_M(rk, true, false)       \
+    PADO_CASE_M(rk, true, true)
+            PADO_CASE(0)
+            PADO_CASE(1)
+            PADO_CASE(2)
+            PADO_CASE(3)
+#undef PADO_CASE
+#undef PADO_CASE_M
+        default: break;
+        }
+    }
+}
 #endif
 
 }  // namespace pado

@@ -85,6 +85,11 @@ StreamFn pick_stream_rk3(bool per, int m, bool xl, int lines, bool adj);
 // solve_bc1/solve_bcn: the closures whose system is solved, when they differ
 // from the right-hand side's (bc1, bcn); SAME_BC: the same.
 constexpr int SAME_BC = 99;
+// Forward apply through the resident tile kernel with plain loads (for fields
+// the streaming kernel's copies cannot move); PADO_E_UNSUPPORTED when the
+// field does not fit it.  info != nullptr: report the plan, launch nothing.
+int launch_resident_single(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb,
+                           int bc1, int bcn, cudaStream_t st, int *info = nullptr);
 int prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
                    int bcn, bool adjoint, int lines, bool no_fast, KParams *kp, bool *trivial, int solve_bc1 = SAME_BC,
                    int solve_bcn = SAME_BC);

@@ -402,3 +402,39 @@ def test_field_operators(torch_cuda):
         for _ in range(2):
             ref = ofil(axis, ref, bc)
     assert rel_err(arr.cpu().numpy(), ref) <= TOL
+
+
+@pytest.mark.parametrize("scheme,kind", OPS)
+def test_parity_resident_plain_loads(torch_cuda, scheme, kind):
+    """Variant 5 -- the resident tiles fed by plain loads, which the automatic
+    choice takes when the streaming kernel's copies cannot move the field (odd
+    extents, unaligned pointers) -- against the oracle, every axis, periodic and
+    bounded, odd and even extents, and an unaligned field."""
+    torch = torch_cuda
+    rng = np.random.default_rng(5 + scheme)
+    for n, shape_of in ((33, lambda n: {1: (5, 7, n), 2: (5, n, 9), 3: (n, 7, 9)}),
+                        (256, lambda n: {1: (3, 4, n), 2: (3, n, 38), 3: (n, 3, 37)})):
+        for periodic in (True, False):
+            op = _make(scheme, n, 0.4, periodic)
+            for variant in (5, 0):
+                op.set_variant(variant)
+                for axis in (1, 2, 3):
+                    shape = shape_of(n)[axis]
+                    f = rng.standard_normal(shape)
+                    for bc1, bcn in ([(0, 0)] if periodic or scheme == oracle.CD06 else [(0, 0), (1, -1)]):
+                        got = _gpu_apply(torch, op, kind, axis, f, bc1, bcn)
+                        ref = _oracle_apply(scheme, kind, axis, f, 0.4, periodic, bc1, bcn)
+                        assert rel_err(got, ref) <= TOL, (n, periodic, variant, axis, bc1, bcn)
+            # an unaligned (odd-offset) field: the automatic choice cannot use TMA
+            op.set_variant(0)
+            shape = (3, 4, n)
+            f = rng.standard_normal(shape)
+            buf = torch.zeros(f.size + 1, dtype=torch.float64, device="cuda")
+            ft = buf[1:].view(shape)
+            ft.copy_(torch.from_numpy(f))
+            out = torch.full((f.size + 1,), float("nan"), dtype=torch.float64, device="cuda")[1:].view(shape)
+            na, nb = na_nb(shape, 1)
+            op.apply(kind, 1, ft, out, na, nb)
+            torch.cuda.synchronize()
+            ref = _oracle_apply(scheme, kind, 1, f, 0.4, periodic, 0, 0)
+            assert rel_err(out.cpu().numpy(), ref) <= TOL
