@@ -216,6 +216,29 @@ __global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) batch_kernel(co
     }
 }
 
+// Asks L2 for the lines of the tile starting at line q0 (all threads, one
+// request per 128-byte line of memory; nothing waits for them).
+__device__ __forceinline__ void prefetch_tile_l2(const KParams &kp, long long q0, bool xl)
+{
+    const long long rem = kp.nlines - q0;
+    if (rem <= 0) return;
+    const int nl = (int)(rem < kp.L ? rem : kp.L), n = kp.n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (xl) {
+        const int chunks = (n * 8 + 127) / 128;
+        for (int i = tid; i < nl * chunks; i += nt) {
+            const double *p = kp.in + (q0 + i / chunks) * (long long)n + (i % chunks) * 16;
+            asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+        }
+    } else {
+        const double *b0 = kp.in + line_base(kp, q0), *b1 = kp.in + line_base(kp, q0 + nl - 1);
+        for (int r = tid; r < n; r += nt) {
+            asm volatile("prefetch.global.L2 [%0];\n" ::"l"(b0 + (long long)r * kp.stride));
+            asm volatile("prefetch.global.L2 [%0];\n" ::"l"(b1 + (long long)r * kp.stride));
+        }
+    }
+}
+
 // One field whose lines the streaming kernel's copy engine cannot move (an odd
 // extent, an unaligned pointer): the same resident tiles with plain loads,
 // the descriptor a kernel parameter, tiles strided over the grid.
@@ -224,9 +247,12 @@ __global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) single_kernel(c
     extern __shared__ double smem_raw[];
     batch_stage(it, batch_carve(it, smem_raw));
     const long long ntiles = (it.kp.nlines + it.kp.L - 1) / it.kp.L;
+    const bool xl = (it.code >> 1) & 1;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         __syncthreads();  // tables staged / the previous tile's buffer free
         const long long q0 = t * it.kp.L;
+        // the next tile of this CTA towards L2 while this one is solved
+        if (t + gridDim.x < ntiles) prefetch_tile_l2(it.kp, (t + gridDim.x) * it.kp.L, xl);
         switch (it.code) {
 #define PADO_CASE_M(rk, per, xl)                                                             \
     case ((rk * 2 + per) * 2 + xl) * 2 + 0: batch_tile<rk, per, 16, xl>(it, smem_raw, q0); break; \
