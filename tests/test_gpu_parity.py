@@ -438,3 +438,28 @@ def test_parity_resident_plain_loads(torch_cuda, scheme, kind):
             torch.cuda.synchronize()
             ref = _oracle_apply(scheme, kind, 1, f, 0.4, periodic, 0, 0)
             assert rel_err(out.cpu().numpy(), ref) <= TOL
+
+
+def test_one_handle_on_two_streams(torch_cuda):
+    """A handle is immutable after init: the same operator applied to two
+    fields on two CUDA streams at once gives each its own correct result."""
+    torch = torch_cuda
+    n = 256
+    rng = np.random.default_rng(21)
+    shape = (n, 8, 64)
+    fa, fb = rng.standard_normal(shape), rng.standard_normal(shape)
+    op = _make(oracle.CD10, n, 0.05, True)
+    ta, tb = torch.from_numpy(fa).cuda(), torch.from_numpy(fb).cuda()
+    oa, ob = torch.empty_like(ta), torch.empty_like(tb)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    na, nb = na_nb(shape, 3)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        with torch.cuda.stream(s1):
+            op.apply(oracle.D1, 3, ta, oa, na, nb)
+        with torch.cuda.stream(s2):
+            op.apply(oracle.D1, 3, tb, ob, na, nb)
+    torch.cuda.synchronize()
+    assert rel_err(oa.cpu().numpy(), _oracle_apply(oracle.CD10, oracle.D1, 3, fa, 0.05, True, 0, 0)) <= TOL
+    assert rel_err(ob.cpu().numpy(), _oracle_apply(oracle.CD10, oracle.D1, 3, fb, 0.05, True, 0, 0)) <= TOL
+    assert op.device_status() == 0
