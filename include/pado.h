@@ -150,8 +150,9 @@ int pado_get_tiling(pado_op_t op, int *m, int *lines);
  * fed by TMA tensor / bulk copies two tiles ahead (needs 16-byte aligned
  * fields, an even x extent for y/z lines and an even n for x lines;
  * PADO_E_UNSUPPORTED otherwise), 5 = the streaming kernel's resident tiles
- * fed by plain loads (any extent and alignment; segments of 16 or 32 rows,
- * i.e. n <= 1024; PADO_E_UNSUPPORTED otherwise).  Adjoints follow the same
+ * fed by plain loads (any extent and alignment; a tile of 8 lines within
+ * 110 KB of shared memory, i.e. n up to about 1400; PADO_E_UNSUPPORTED
+ * otherwise).  Adjoints follow the same
  * choice (4 runs the transposed sweep in the tile, then B^T); 2, 3 and 5
  * mean 1 for adjoints.
  * No counterpart in the reference (a B200 tuning knob). */

@@ -59,7 +59,7 @@ bool resident_fallback(const pado_op_s *op, int axis) { return axis == 1 || op->
 // Default tiling: segment length and lines per CTA for a line of length n.
 void default_tiling(int n, int *m, int *lines)
 {
-    *m = n > 32 * 32 ? 64 : (n >= 96 ? 32 : 16);
+    *m = n >= 32 * 32 ? 64 : (n >= 96 ? 32 : 16);
     const int S = (n + *m - 1) / *m;
     int L = 32;
     while (L > 8 && L * S > max_threads_for_m(*m)) L /= 2;

@@ -50,7 +50,7 @@ int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d,
 {
     *skip = false;
     if (!it.op) return PADO_E_NULL;
-    if (it.op->m != 16 && it.op->m != 32) return PADO_E_SIZE;  // batch kernels are built for 16- and 32-row segments
+    if (it.op->m != 16 && it.op->m != 32 && it.op->m != 64) return PADO_E_SIZE;  // the segment lengths built
     if (it.axis < 1 || it.axis > 3 || it.n1 < 0 || it.n2 < 0 || it.n3 < 0) return PADO_E_ARG;
     const long long ext[3] = {it.n1, it.n2, it.n3};
     if (ext[it.axis - 1] != it.op->n) return PADO_E_ARG;
@@ -109,8 +109,8 @@ int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d,
 }
 
 // The resident single-field kernel (single_kernel) for one apply; returns
-// PADO_E_UNSUPPORTED when the field does not fit its rules (segments of 16 or
-// 32 rows, the tile within the shared-memory cap), so that the caller can use
+// PADO_E_UNSUPPORTED when the field does not fit its rules (segments of 16,
+// 32 or 64 rows, the tile within the shared-memory cap), so that the caller can use
 // the line kernel instead.  info (not null): fill the launch plan the way
 // pado_launch_plan reports it and launch nothing.
 int launch_resident_single(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb,

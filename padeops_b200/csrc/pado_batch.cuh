@@ -31,14 +31,15 @@ struct BatchItemDev {
     const double *rtab;    // border responses
     const int *toff;       // first table row of each segment
     long long tile0;       // first tile index of this item
-    int code;              // ((rk * 2 + periodic) * 2 + x lines) * 2 + (segment length 32)
+    int code;              // ((rk * 2 + periodic) * 2 + x lines) * 4 + (0, 1, 2: segments of 16, 32, 64 rows)
     int etab_rows, ktab_rows, pad;
 };
 
 PADO_HD PADO_INLINE int batch_code(int rk, bool periodic, bool xl, int m)
 {
-    return ((rk * 2 + (periodic ? 1 : 0)) * 2 + (xl ? 1 : 0)) * 2 + (m == 32 ? 1 : 0);
+    return ((rk * 2 + (periodic ? 1 : 0)) * 2 + (xl ? 1 : 0)) * 4 + (m == 64 ? 2 : (m == 32 ? 1 : 0));
 }
+PADO_HD PADO_INLINE bool batch_code_xl(int code) { return (code >> 2) & 1; }
 
 // Shared memory of a batch tile (doubles): the item's staged tables (etab,
 // ktab, rtab, toff), then the summaries, border slots, border weights,
@@ -198,8 +199,9 @@ __global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) batch_kernel(co
         const long long q0 = (t - it.tile0) * it.kp.L;
         switch (it.code) {
 #define PADO_CASE_M(rk, per, xl)                                                             \
-    case ((rk * 2 + per) * 2 + xl) * 2 + 0: batch_tile<rk, per, 16, xl>(it, smem_raw, q0); break; \
-    case ((rk * 2 + per) * 2 + xl) * 2 + 1: batch_tile<rk, per, 32, xl>(it, smem_raw, q0); break;
+    case ((rk * 2 + per) * 2 + xl) * 4 + 0: batch_tile<rk, per, 16, xl>(it, smem_raw, q0); break; \
+    case ((rk * 2 + per) * 2 + xl) * 4 + 1: batch_tile<rk, per, 32, xl>(it, smem_raw, q0); break; \
+    case ((rk * 2 + per) * 2 + xl) * 4 + 2: batch_tile<rk, per, 64, xl>(it, smem_raw, q0); break;
 #define PADO_CASE(rk)                  \
     PADO_CASE_M(rk, false, false)      \
     PADO_CASE_M(rk, false, true)       \
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) single_kernel(c
     extern __shared__ double smem_raw[];
     batch_stage(it, batch_carve(it, smem_raw));
     const long long ntiles = (it.kp.nlines + it.kp.L - 1) / it.kp.L;
-    const bool xl = (it.code >> 1) & 1;
+    const bool xl = batch_code_xl(it.code);
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         __syncthreads();  // tables staged / the previous tile's buffer free
         const long long q0 = t * it.kp.L;
@@ -255,8 +257,9 @@ __global__ void __launch_bounds__(BATCH_THREADS, BATCH_MIN_CTAS) single_kernel(c
         if (t + gridDim.x < ntiles) prefetch_tile_l2(it.kp, (t + gridDim.x) * it.kp.L, xl);
         switch (it.code) {
 #define PADO_CASE_M(rk, per, xl)                                                             \
-    case ((rk * 2 + per) * 2 + xl) * 2 + 0: batch_tile<rk, per, 16, xl>(it, smem_raw, q0); break; \
-    case ((rk * 2 + per) * 2 + xl) * 2 + 1: batch_tile<rk, per, 32, xl>(it, smem_raw, q0); break;
+    case ((rk * 2 + per) * 2 + xl) * 4 + 0: batch_tile<rk, per, 16, xl>(it, smem_raw, q0); break; \
+    case ((rk * 2 + per) * 2 + xl) * 4 + 1: batch_tile<rk, per, 32, xl>(it, smem_raw, q0); break; \
+    case ((rk * 2 + per) * 2 + xl) * 4 + 2: batch_tile<rk, per, 64, xl>(it, smem_raw, q0); break;
 #define PADO_CASE(rk)                  \
     PADO_CASE_M(rk, false, false)      \
     PADO_CASE_M(rk, false, true)       \
