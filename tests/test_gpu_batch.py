@@ -71,6 +71,42 @@ def test_batch_parity(mode):
     b.destroy()
 
 
+@pytest.mark.parametrize("mode", ["run", "run_graph"])
+def test_batch_long_lines(mode):
+    """Items whose lines are 1024 points long (segments of 64 rows), every
+    scheme, axis and boundary type, mixed with short ones in one batch."""
+    import torch
+
+    import padeops_b200 as pb
+    from padeops_b200.batch import Batch
+
+    rng = np.random.default_rng(17)
+    items, host = [], []
+    n = 1024
+    for scheme, kind in ((oracle.CD06, oracle.D1), (oracle.CD10, oracle.D1), (oracle.CD10, oracle.D2),
+                         (oracle.CF90, oracle.FILTER)):
+        for periodic in (True, False):
+            dx = 2 * np.pi / n if periodic else 1.0 / (n - 1)
+            op = {oracle.CD06: pb.cd06, oracle.CD10: pb.cd10, oracle.CF90: pb.cf90}[scheme]()
+            assert (op.init(n, periodic) if scheme == oracle.CF90 else op.init(n, dx, periodic, 0, 0)) == 0
+            for axis, shape in ((1, (3, 5, n)), (2, (3, n, 8)), (3, (n, 3, 8))):
+                bc1, bcn = (0, 0) if periodic or scheme == oracle.CD06 else (1, -1)
+                f = rng.standard_normal(shape)
+                ft = torch.from_numpy(f).cuda()
+                items.append((op, kind, axis, ft, torch.full_like(ft, float("nan")), bc1, bcn))
+                host.append((scheme, kind, n, dx, periodic, (0, 0), bc1, bcn, axis, f))
+    short, short_host = _items(torch, 8, seed=23)
+    items += short
+    host += short_host
+    b = Batch(items)
+    for _ in range(2):
+        for it in items:
+            it[4].fill_(float("nan"))
+        getattr(b, mode)()
+        _check(torch, items, host)
+    b.destroy()
+
+
 def test_batch_96_uneven_fields():
     """The 96-field uneven workload shape (dimensions drawn from the configs'
     set, capped at 128 here to keep the oracle quick)."""

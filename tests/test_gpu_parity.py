@@ -409,11 +409,13 @@ def test_parity_resident_plain_loads(torch_cuda, scheme, kind):
     """Variant 5 -- the resident tiles fed by plain loads, which the automatic
     choice takes when the streaming kernel's copies cannot move the field (odd
     extents, unaligned pointers) -- against the oracle, every axis, periodic and
-    bounded, odd and even extents, and an unaligned field."""
+    bounded, odd and even extents, segments of 16, 32 and 64 rows, and an
+    unaligned field."""
     torch = torch_cuda
     rng = np.random.default_rng(5 + scheme)
     for n, shape_of in ((33, lambda n: {1: (5, 7, n), 2: (5, n, 9), 3: (n, 7, 9)}),
-                        (256, lambda n: {1: (3, 4, n), 2: (3, n, 38), 3: (n, 3, 37)})):
+                        (256, lambda n: {1: (3, 4, n), 2: (3, n, 38), 3: (n, 3, 37)}),
+                        (1024, lambda n: {1: (3, 4, n), 2: (3, n, 7), 3: (n, 3, 7)})):  # 64-row segments
         for periodic in (True, False):
             op = _make(scheme, n, 0.4, periodic)
             for variant in (5, 0):
