@@ -151,7 +151,7 @@ int pado_get_tiling(pado_op_t op, int *m, int *lines);
  * fields, an even x extent for y/z lines and an even n for x lines;
  * PADO_E_UNSUPPORTED otherwise), 5 = the streaming kernel's resident tiles
  * fed by plain loads (any extent and alignment; a tile of 8 lines within
- * 110 KB of shared memory, i.e. n up to about 1400; PADO_E_UNSUPPORTED
+ * 110 KB of shared memory, i.e. n up to about 1300; PADO_E_UNSUPPORTED
  * otherwise).  Adjoints follow the same
  * choice (4 runs the transposed sweep in the tile, then B^T); 2, 3 and 5
  * mean 1 for adjoints.
@@ -190,6 +190,9 @@ typedef struct {
     double *df;
 } pado_batch_item;
 
+/* PADO_E_SIZE when an item's tile of 8 lines does not fit the persistent
+ * kernel's 110 KB of shared memory (lines longer than about 1300 points);
+ * such fields go through pado_apply. */
 int pado_batch_create(pado_batch_t *batch, const pado_batch_item *items, int nitems);
 /* Enqueue the whole batch on `stream` as one persistent kernel launch. */
 int pado_batch_run(pado_batch_t batch, void *stream);
