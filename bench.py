@@ -417,7 +417,7 @@ def run_batch_profile(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pado", choices=["pado", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
