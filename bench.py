@@ -71,18 +71,60 @@ def profiled_traffic() -> float | None:
 
 
 class ClockSampler:
-    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+    """Samples the SM clock, its maximum and the clock-event (throttle) reasons
+    while running: NVML read directly every 10 ms (so that a timed region of
+    tens of milliseconds still gets samples), else nvidia-smi every 100 ms.
+    Reads only; changes no setting of the GPU."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
         self.lines: list[str] = []
+        self.samples: list[tuple[float, float, set]] = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            prop = torch.cuda.get_device_properties(self.index)
+            bus = f"{prop.pci_domain_id:08x}:{prop.pci_bus_id:02x}:{prop.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self, nv, h):
+        bits = [getattr(nv, "nvmlClocksEventReason" + k, getattr(nv, "nvmlClocksThrottleReason" + k, 0))
+                for k in ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
+        reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                             getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self.stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                act = int(reasons_fn(h)) if reasons_fn else 0
+                self.samples.append((sm, mx, {n for n, b in zip(self.NAMES, bits) if b and act & b}))
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.nvml = nv
+            self.t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -103,6 +145,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml:
+            self.t.join(timeout=1.0)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -112,7 +161,10 @@ class ClockSampler:
 
     def summary(self) -> dict:
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for a, b, r in self.samples:
+            sm.append(a)
+            mx.append(b)
+            reasons |= r
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
@@ -122,11 +174,11 @@ class ClockSampler:
                 mx.append(float(parts[1]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[4:8]):
+            for nm, v in zip(self.NAMES, parts[4:8]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def make_field(seed: int) -> np.ndarray:
