@@ -1,9 +1,10 @@
 """Writes the golden fixtures of tests/golden (run from the repository root:
 ``python tests/golden/make_golden.py``).
 
-* ``recipes.json``: max |D f - exact| of the reference tests' recipes
-  (tests/test_cd06.F90, test_cd10_NP.F90, test_cd10_der2.F90, test_cf90.F90)
-  evaluated through the oracle.
+* ``recipes.json``: the error each reference test prints (tests/test_cd06.F90,
+  test_cd10.F90, test_cd10_NP.F90, test_cd10_der2.F90, test_cf90.F90,
+  test_filters.F90, test_filters_NP.F90, replayed as written by
+  tests/recipes.py), evaluated through the oracle.
 * ``oracle_small.npz``: seeded small fields and the oracle's outputs for every
   operator, both boundary kinds, every closure pair and all three axes.  The
   GPU parity tests compare the CUDA kernels with these arrays (so a GPU run

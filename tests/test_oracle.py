@@ -8,9 +8,17 @@ nothing), so the restatement is pinned by:
   transfer function of src/utilities/spectral.F90:938-1010 predicts;
 * an independent dense assembly of the same operators (oracle/dense.py),
   bounded closures and all boundary specifications included;
-* replays of the reference tests' recipes (tests/test_cd06.F90,
-  test_cd10_NP.F90, test_cd10_der2.F90, test_cf90.F90): same grids,
-  functions, closures, with the error against the exact derivative bounded;
+* replays of the reference tests as written (tests/test_cd06.F90,
+  test_cd10.F90, test_cd10_NP.F90, test_cd10_der2.F90, test_cf90.F90,
+  test_filters.F90, test_filters_NP.F90): same sizes, grids, functions,
+  closures and printed errors; where the discrete answer is known in closed
+  form (periodic modes, modes with the parity of symmetric / antisymmetric
+  closures) it is checked to rounding, and the other printed errors are
+  recorded in tests/golden/recipes.json;
+* closed-form known answers for every bounded closure pair: polynomials up to
+  each closure's formal order and boundary-parity Fourier modes are
+  reproduced exactly, and a planted 1e-7 error in any closure coefficient of
+  the dense transcription breaks them;
 * the init error codes of the reference (cd06.F90:153-183,
   cd10.F90:219-309, cf90.F90:123-168) and the n == 1 cases.
 
@@ -26,7 +34,7 @@ import pytest
 import oracle
 from oracle import dense
 from tests.fields import na_nb, rel_err
-from tests.recipes import mod_wavenumber, recipe_errors
+from tests.recipes import closure_pins, mod_wavenumber, oracle_apply, pin_tolerance, reference_recipes
 
 OPS = [(oracle.CD06, oracle.D1), (oracle.CD10, oracle.D1), (oracle.CD10, oracle.D2), (oracle.CF90, oracle.FILTER)]
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -110,17 +118,72 @@ def test_matches_dense_assembly(scheme, kind, periodic, n):
 
 
 def test_reference_test_recipes():
-    """Replays of the reference tests: the error against the exact derivative
-    is at rounding level for every recipe (<= 1e-12; a wrong coefficient gives
-    errors of 1e-4 and more), and equals what tests/golden/recipes.json recorded
-    (within 1e-13)."""
+    """The reference tests replayed as written.  Where the discrete operator's
+    answer is known in closed form (periodic Fourier modes; test_cd10_NP's
+    cos x with closures (1, -1); test_filters_NP's sin x with closures
+    (-1, -1)) the oracle matches it to <= 1e-12.  Every printed error equals
+    what tests/golden/recipes.json recorded (1e-13 absolute + 1e-9 relative):
+    for test_cd10_der2 and test_cf90, whose bc (0, 0) closures have truncation
+    errors, that record is the pin of the closure rows' values."""
     with open(os.path.join(GOLDEN, "recipes.json")) as fh:
         recorded = json.load(fh)
-    got = recipe_errors()
-    assert set(got) == set(recorded)
-    for name, err in got.items():
-        assert err <= 1e-12, (name, err)
-        assert abs(err - recorded[name]) <= 1e-13, (name, err, recorded[name])
+    seen = set()
+    for c in reference_recipes():
+        got = oracle_apply(c)
+        seen.add(c.name)
+        if c.closed is not None:
+            assert c.closed_err(got) <= 1e-12, (c.name, c.source, c.closed_err(got))
+        err = c.printed(got)
+        assert abs(err - recorded[c.name]) <= 1e-13 + 1e-9 * abs(recorded[c.name]), (c.name, err, recorded[c.name])
+    assert seen == set(recorded)
+
+
+@pytest.mark.parametrize("n", [16, 40])
+def test_closure_pins(n):
+    """Every bounded closure pair of cd10 d1, cd10 d2 and cf90 (cd06: (0, 0)),
+    along every axis: polynomials up to the closure's formal order and
+    boundary-parity Fourier modes are reproduced exactly (tolerance
+    ``pin_tolerance``: 1e-12, or 1e-14 n^2 for second derivatives)."""
+    count = 0
+    for c in closure_pins(n=n):
+        err = c.closed_err(oracle_apply(c))
+        assert err <= pin_tolerance(c), (c.name, err)
+        count += 1
+    assert count == 3 * (1 + 9 + 9 + 9)
+
+
+# closure coefficients of the dense transcription, per operator; the row
+# weights w1..w4 are left out (they scale both sides of a row and cancel), as
+# are the interior constants the closures are derived from at import time
+_PLANT = [("_c6", (oracle.CD06, oracle.D1), ["alpha", "p", "q", "r", "s", "qp", "ap", "app", "qpp", "rpp"]),
+          ("_k", (oracle.CD10, oracle.D1), ["alpha", "p", "q", "r", "s", "qp", "ap", "appp", "bppp", "qppp", "rppp",
+                                            "sppp", "app", "bpp", "qpp", "rpp"]),
+          ("_d2b", (oracle.CD10, oracle.D2), ["a1", "b1", "c1", "d1", "al1", "al2", "a2", "al3", "be3", "a3", "b3"]),
+          ("CF2", (oracle.CF90, oracle.FILTER), ["al", "a", "b"]),
+          ("CF3", (oracle.CF90, oracle.FILTER), ["al", "be", "a", "b", "c"]),
+          ("CF4", (oracle.CF90, oracle.FILTER), ["al", "be", "a", "b", "c", "d"])]
+
+
+@pytest.mark.parametrize("table,op,keys", _PLANT, ids=[p[0] for p in _PLANT])
+def test_pins_catch_planted_closure_errors(table, op, keys, monkeypatch):
+    """The closure pins are discriminating: a relative error of 1e-7 planted in
+    any closure coefficient of the dense transcription (oracle/dense.py) makes
+    them fail by more than 10x their tolerance."""
+    checks = [c for c in closure_pins(n=40) if (c.scheme, c.kind) == op and c.axis == 1]
+
+    def worst():
+        w = 0.0
+        for c in checks:
+            D = dense.operator(c.scheme, c.kind, c.n, c.dx, c.periodic, *c.bc)
+            w = max(w, c.closed_err(dense.apply_axis(D, c.f, c.axis)) / pin_tolerance(c))
+        return w
+
+    assert worst() <= 1.0
+    d = getattr(dense, table)
+    for key in keys:
+        with monkeypatch.context() as m:
+            m.setitem(d, key, d[key] * (1 + 1e-7))
+            assert worst() > 10.0, (table, key)
 
 
 def test_init_errors_and_n1():
