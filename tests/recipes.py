@@ -130,7 +130,9 @@ def _axes(nx, ny, nz, dx, dy, dz):
 
 
 def _full(a, shape):
-    return np.ascontiguousarray(np.broadcast_to(a, shape), dtype=np.float64)
+    out = np.empty(shape)
+    out[...] = a
+    return out
 
 
 def reference_recipes(large: bool = True) -> Iterator[Check]:
@@ -304,10 +306,15 @@ def _mode_pin(scheme, kind, n, bc1, bcn):
 
 
 def pin_tolerance(c: Check) -> float:
-    """Rounding bound of a closed-form pin: 1e-12 for first derivatives and the
-    filter; a second derivative of a polynomial loses digits in proportion to
-    1/dx^2, i.e. n^2 on a fixed interval, so 1e-14 n^2 (1.6e-11 at n = 40)."""
-    return 1e-14 * c.n ** 2 if c.kind == D2 else 1e-12
+    """Rounding bound of a closed-form pin on a fixed interval: a first
+    derivative loses digits in proportion to 1/dx, i.e. n (max(1e-12, 4e-15 n):
+    1e-12 up to n = 250), a second derivative in proportion to n^2 (1e-14 n^2,
+    1.6e-11 at n = 40), the filter none (1e-12)."""
+    if c.kind == D2:
+        return 1e-14 * c.n ** 2
+    if c.kind == D1:
+        return max(1e-12, 4e-15 * c.n)
+    return 1e-12
 
 
 def closure_pins(n: int = 40, lines: int = 3, seed: int = 11) -> Iterator[Check]:
