@@ -17,10 +17,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpado.so")
-SOURCES = ["pado_api.cu", "pado_batch.cu", "pado_tables.cpp", "pado_inst_rk0.cu", "pado_inst_rk1.cu",
-           "pado_inst_rk2.cu", "pado_inst_rk3.cu"]
+SOURCES = ["pado_api.cu", "pado_batch.cu", "pado_tables.cpp", "pado_inst.cu"]
 HEADERS = ["pado_common.h", "pado_tables.h", "pado_kernels.cuh", "pado_batch.cuh", "pado_internal.h", "pado_params.h",
            "pado_stream.cuh", "pado_resident.cuh"]
+# pado_inst.cu is compiled once per stencil (-DPADO_RK=n) into pado_inst_rkN.o
+STENCILS = 4
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr"]
@@ -55,12 +56,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 return LIB
     objs = []
     procs = []
+    units = []
     for src in SOURCES:
+        stem = os.path.splitext(src)[0]
+        if src == "pado_inst.cu":
+            units += [(src, f"{stem}_rk{rk}.o", [f"-DPADO_RK={rk}"]) for rk in range(STENCILS)]
+        else:
+            units.append((src, stem + ".o", []))
+    for src, oname, defs in units:
         path = os.path.join(CSRC, src)
-        if not os.path.exists(path):
-            continue
-        obj = os.path.join(LIBDIR, os.path.splitext(src)[0] + ".o")
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", os.path.join(HERE, "..", "include"), "-c", path, "-o", obj]
+        obj = os.path.join(LIBDIR, oname)
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *defs, "-I", os.path.join(HERE, "..", "include"), "-c", path, "-o", obj]
         if verbose:
             cmd.append("-Xptxas=-v")
         procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

@@ -1,10 +1,21 @@
-// pado_inst_rk2.cu -- instantiations of the line kernels for one stencil
-// (cd10 second derivative); split per stencil so the library compiles in parallel.
+// pado_inst.cu -- instantiations of the line and streaming kernels for one
+// stencil.  The library compiles this file once per stencil with
+// -DPADO_RK=0..3 (cd06 d1, cd10 d1, cd10 d2, cf90), so the four instantiation
+// sets build in parallel; each defines the entry points pick_kernel_rkN and
+// pick_stream_rkN of pado_internal.h.
 #include "pado_internal.h"
+
+#ifndef PADO_RK
+#error "compile with -DPADO_RK=<stencil 0..3>"
+#endif
+#define PADO_CAT2(a, b) a##b
+#define PADO_CAT(a, b) PADO_CAT2(a, b)
 
 namespace pado {
 
 namespace {
+
+constexpr int RK = PADO_RK;
 
 // variant 1: one CTA per tile; 2: persistent CTAs with cp.async prefetch;
 // 3: persistent CTAs reading straight from global memory with an L2 prefetch.
@@ -12,7 +23,6 @@ namespace {
 template <bool PER, int M>
 KernelFn pick_in(bool adj, bool contiguous, int variant)
 {
-    constexpr int RK = 2;
     if (adj) return contiguous ? line_kernel<RK, PER, true, M, IN_LINES> : line_kernel<RK, PER, true, M, IN_GLOBAL>;
     if (variant == 2)
         return contiguous ? line_kernel_persist<RK, PER, M, IN_LINES> : line_kernel_persist<RK, PER, M, IN_ROWS>;
@@ -33,7 +43,6 @@ KernelFn pick_m(int m, bool adj, bool contiguous, int variant)
 template <bool PER, bool XL, int LT, bool ADJ>
 StreamFn pick_stream_m(int m)
 {
-    constexpr int RK = 2;
     switch (m) {
     case 16: return stream_kernel<RK, PER, 16, XL, LT, ADJ>;
     case 32: return stream_kernel<RK, PER, 32, XL, LT, ADJ>;
@@ -50,13 +59,13 @@ StreamFn pick_stream_l(int m, bool xl, int lines)
 
 }  // namespace
 
-StreamFn pick_stream_rk2(bool per, int m, bool xl, int lines, bool adj)
+StreamFn PADO_CAT(pick_stream_rk, PADO_RK)(bool per, int m, bool xl, int lines, bool adj)
 {
     if (adj) return per ? pick_stream_l<true, true>(m, xl, lines) : pick_stream_l<false, true>(m, xl, lines);
     return per ? pick_stream_l<true, false>(m, xl, lines) : pick_stream_l<false, false>(m, xl, lines);
 }
 
-KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant)
+KernelFn PADO_CAT(pick_kernel_rk, PADO_RK)(bool per, bool adj, bool contiguous, int m, int variant)
 {
     return per ? pick_m<true>(m, adj, contiguous, variant) : pick_m<false>(m, adj, contiguous, variant);
 }

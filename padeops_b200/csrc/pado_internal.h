@@ -66,7 +66,8 @@ namespace pado {
 // Validates an apply request and fills the launch parameters for the given
 // lines-per-CTA.  Returns PADO_OK, or an error; *trivial is set when n == 1
 // or the field is empty (nothing for a line kernel to do).
-// Line-kernel entry points, one translation unit per stencil (pado_inst_rk*.cu).
+// Kernel entry points, one translation unit per stencil (pado_inst.cu built
+// with -DPADO_RK=0..3).
 using KernelFn = void (*)(const KParams);
 KernelFn pick_kernel_rk0(bool per, bool adj, bool contiguous, int m, int variant);
 KernelFn pick_kernel_rk1(bool per, bool adj, bool contiguous, int m, int variant);
