@@ -109,6 +109,18 @@ int pado_filter3(pado_op_t op, const double *f, double *df, long na, long nb, in
 int pado_apply(pado_op_t op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1, int bcn,
                void *stream);
 
+/* Scaled / accumulating form of pado_apply: df = alpha * D f + beta * df,
+ * beta 0 or 1 (else PADO_E_ARG).  With beta = 1 a field operator sums its
+ * terms straight into its output -- laplacian = d2d1 + d2d2 + d2d3 as three
+ * calls (cgrid.F90:480-517), a curl component as a derivative minus another
+ * (operators.F90:58-97) -- reading df once per call instead of through a
+ * temporary (24 bytes per point instead of 16 + 24).  Same arguments, errors
+ * and stream semantics as pado_apply; f and df must not overlap.  No
+ * counterpart in the reference (the solver's callers sum derivatives into
+ * temporaries). */
+int pado_apply_scaled(pado_op_t op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
+                      int bcn, double alpha, double beta, void *stream);
+
 /* Adjoint (transpose) of pado_apply: fbar = D^T g with D = A^{-1} B the
  * operator pado_apply applies, boundary closures included.  No counterpart in
  * the reference; used for reverse-mode differentiation. */

@@ -52,6 +52,7 @@ SIGNATURES = {
     "pado_filter1": (_I, _APPLY), "pado_filter2": (_I, _APPLY), "pado_filter3": (_I, _APPLY),
     "pado_apply": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, _P]),
     "pado_apply_adjoint": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, _P]),
+    "pado_apply_scaled": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, _D, _D, _P]),
     "pado_apply_host": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, _P]),
     "pado_set_tiling": (_I, [_P, _I, _I]),
     "pado_set_kernel_variant": (_I, [_P, _I]),

@@ -318,7 +318,7 @@ int launch_stream(pado_op_s *op, const StreamParams &sp, bool adj, int threads, 
 
 int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
                          int bcn, bool adjoint, int lines, bool no_fast, KParams *kpo, bool *trivial, int solve_bc1,
-                         int solve_bcn)
+                         int solve_bcn, int out_mode, double out_alpha)
 {
     *trivial = true;
     if (!op) return PADO_E_NULL;
@@ -343,6 +343,8 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
     fill_params(kp, dt.host, n, op->scheme == CD06 ? op->bc1 : bc1, op->scheme == CD06 ? op->bcn : bcn);
     kp.in = f;
     kp.out = df;
+    kp.out_mode = out_mode;
+    kp.out_alpha = out_alpha;
     set_geometry(kp, axis, n, na, nb);
     kp.L = lines;
     kp.tab = dt.tab;
@@ -366,20 +368,40 @@ int pado::prepare_launch(pado_op_s *op, int kind, int axis, const double *f, dou
 
 namespace {
 
-int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1, int bcn,
-           cudaStream_t st, bool adjoint, int solve_bc1 = SAME_BC, int solve_bcn = SAME_BC)
+// df = alpha * f (+ df) elementwise: the n == 1 filter under a scaled or
+// accumulating output mode
+__global__ void out_copy_kernel(const double *__restrict__ f, double *__restrict__ df, long long total, int mode,
+                                double alpha)
 {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
+        df[i] = mode == OUT_ACC ? fma(alpha, f[i], df[i]) : alpha * f[i];
+}
+
+int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1, int bcn,
+           cudaStream_t st, bool adjoint, int solve_bc1 = SAME_BC, int solve_bcn = SAME_BC, int out_mode = OUT_STORE,
+           double out_alpha = 1.0)
+{
+    if (adjoint && out_mode != OUT_STORE) return PADO_E_UNSUPPORTED;
     KParams kp;
     bool trivial = true;
     int rc = prepare_launch(op, kind, axis, f, df, na, nb, bc1, bcn, adjoint, op ? op->lines : 0, false, &kp, &trivial,
-                            solve_bc1, solve_bcn);
+                            solve_bc1, solve_bcn, out_mode, out_alpha);
     if (rc != PADO_OK) return rc;
     if (trivial) {
         const long long total = (long long)op->n * na * nb;
         if (total == 0) return PADO_OK;
         // n == 1: cd06.F90:781-784, cd10.F90:2037-2040 (zero), cf90.F90:1028-1031 (copy)
-        cudaError_t e = (kind == FILTER) ? cudaMemcpyAsync(df, f, total * sizeof(double), cudaMemcpyDeviceToDevice, st)
-                                         : cudaMemsetAsync(df, 0, total * sizeof(double), st);
+        cudaError_t e = cudaSuccess;
+        if (kind != FILTER) {
+            if (out_mode != OUT_ACC) e = cudaMemsetAsync(df, 0, total * sizeof(double), st);  // df + alpha * 0 = df
+        } else if (out_mode == OUT_STORE) {
+            e = cudaMemcpyAsync(df, f, total * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        } else {
+            const long long blocks = std::min<long long>((total + 255) / 256, 4096);
+            out_copy_kernel<<<(unsigned)blocks, 256, 0, st>>>(f, df, total, out_mode, out_alpha);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+            e = cudaGetLastError();
+        }
         return e == cudaSuccess ? PADO_OK : cuda_fail(e);
     }
     if (op->variant == 0 || op->variant == 4) {
@@ -395,7 +417,7 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
     }
     if ((op->variant == 5 || (op->variant == 0 && resident_fallback(op, axis))) && !adjoint && solve_bc1 == SAME_BC) {
         // the same resident tiles, with plain loads
-        rc = launch_resident_single(op, kind, axis, f, df, na, nb, bc1, bcn, st);
+        rc = launch_resident_single(op, kind, axis, f, df, na, nb, bc1, bcn, st, nullptr, out_mode, out_alpha);
         if (rc != PADO_E_UNSUPPORTED || op->variant == 5) return rc;
     }
     // lines per CTA: the handle's choice, halved until the segments fit
@@ -509,6 +531,14 @@ int pado_apply(pado_op_t op, int kind, int axis, const double *f, double *df, lo
                void *stream)
 {
     return launch(op, kind, axis, f, df, na, nb, bc1, bcn, (cudaStream_t)stream, false);
+}
+
+int pado_apply_scaled(pado_op_t op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
+                      int bcn, double alpha, double beta, void *stream)
+{
+    if (beta != 0.0 && beta != 1.0) return PADO_E_ARG;
+    const int mode = beta == 1.0 ? OUT_ACC : (alpha == 1.0 ? OUT_STORE : OUT_SCALE);
+    return launch(op, kind, axis, f, df, na, nb, bc1, bcn, (cudaStream_t)stream, false, SAME_BC, SAME_BC, mode, alpha);
 }
 
 int pado_apply_adjoint(pado_op_t op, int kind, int axis, const double *g, double *fbar, long na, long nb, int bc1,

@@ -114,7 +114,7 @@ int batch_item_descriptor(const pado_batch_item &it, int lines, BatchItemDev *d,
 // the line kernel instead.  info (not null): fill the launch plan the way
 // pado_launch_plan reports it and launch nothing.
 int launch_resident_single(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb,
-                           int bc1, int bcn, cudaStream_t st, int *info)
+                           int bc1, int bcn, cudaStream_t st, int *info, int out_mode, double out_alpha)
 {
     pado_batch_item it{};
     it.op = op;
@@ -136,6 +136,8 @@ int launch_resident_single(pado_op_s *op, int kind, int axis, const double *f, d
     if (rc == PADO_E_SIZE) return PADO_E_UNSUPPORTED;
     if (rc != PADO_OK || skip) return rc;
     d.tile0 = 0;
+    d.kp.out_mode = out_mode;
+    d.kp.out_alpha = out_alpha;
     cudaError_t e = cudaFuncSetAttribute((const void *)single_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)BATCH_SMEM_CAP);
     if (e != cudaSuccess) return cuda_fail(e);

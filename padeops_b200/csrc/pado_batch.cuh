@@ -142,12 +142,16 @@ __device__ __noinline__ void batch_tile(const BatchItemDev &it, double *smem, lo
         for (int ll = warp; ll < nl; ll += nw) {
             double *dst = kp.out + (q0 + ll) * (long long)n;
             const double *src = sm.tile + (size_t)ll * P;
-            for (int r = lane; r < n; r += 32) __stcs(dst + r, src[r]);
+            if (kp.out_mode == OUT_STORE) {
+                for (int r = lane; r < n; r += 32) __stcs(dst + r, src[r]);
+            } else {
+                for (int r = lane; r < n; r += 32) out_put(kp, dst + r, src[r]);
+            }
         }
     } else {
         const bool live = l < nl;
         double *dst = kp.out + (live ? line_base(kp, q0 + l) : 0);
-        if (active) RL::template fin<true>(kp, sm, line, rs, l, s, dst, kp.stride, live);
+        if (active) RL::template fin<true>(kp, sm, line, rs, l, s, dst, kp.stride, live, true);
     }
 }
 

@@ -89,10 +89,12 @@ constexpr int SAME_BC = 99;
 // Forward apply through the resident tile kernel with plain loads (for fields
 // the streaming kernel's copies cannot move); PADO_E_UNSUPPORTED when the
 // field does not fit it.  info != nullptr: report the plan, launch nothing.
+// out_mode / out_alpha: how results reach df (OutMode of pado_kernels.cuh).
 int launch_resident_single(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb,
-                           int bc1, int bcn, cudaStream_t st, int *info = nullptr);
+                           int bc1, int bcn, cudaStream_t st, int *info = nullptr, int out_mode = OUT_STORE,
+                           double out_alpha = 1.0);
 int prepare_launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,
                    int bcn, bool adjoint, int lines, bool no_fast, KParams *kp, bool *trivial, int solve_bc1 = SAME_BC,
-                   int solve_bcn = SAME_BC);
+                   int solve_bcn = SAME_BC, int out_mode = OUT_STORE, double out_alpha = 1.0);
 
 }  // namespace pado

@@ -74,7 +74,21 @@ struct KParams {
     unsigned short xof[32], xob[32]; // first xtab block of each segment's forward / backward list
     const double *rtab;    // cyclic: (R1, R2) per row for rows [0, ie) then [je, nb) (streaming kernel)
     int ie, je;
+    // how results reach df (OutMode): stored, scaled by out_alpha, or
+    // out_alpha * result added to df
+    int out_mode;
+    double out_alpha;
 };
+
+enum OutMode { OUT_STORE = 0, OUT_SCALE = 1, OUT_ACC = 2 };
+
+// One result x to its place p in df, through the launch's output mode.
+PADO_HD PADO_INLINE void out_put(const KParams &kp, double *p, double x)
+{
+    if (kp.out_mode == OUT_ACC) *p = fma(kp.out_alpha, x, *p);
+    else if (kp.out_mode == OUT_SCALE) *p = kp.out_alpha * x;
+    else *p = x;
+}
 
 // Staged response row of banded row i (i < ie or i >= je).
 PADO_HD PADO_INLINE const double *resp_row(const KParams &kp, const double *rtab, int i)
@@ -149,6 +163,7 @@ struct LineIO {
     double *dst;
     long long ds;
     bool live;
+    bool tile = false;  // dst is the shared-memory tile (results reach df later)
 };
 
 // Per-thread segment values: M rows plus the 8-row stencil window margin.
@@ -217,7 +232,7 @@ PADO_HD PADO_INLINE void tile_store(const KParams &kp, const Smem &sm, long long
     int l = tid / n, r = tid - (tid / n) * n;
     const int dl = nthreads / n, dr = nthreads - dl * n;
     for (int e = tid; e < total; e += nthreads) {
-        dst[e] = sm.tile[(size_t)l * P + r];
+        out_put(kp, dst + e, sm.tile[(size_t)l * P + r]);
         l += dl;
         r += dr;
         if (r >= n) {
@@ -418,6 +433,16 @@ struct LineKernel {
         const double de = kp.kc[6];
         const double Q1 = st[0], Q2 = st[kp.L];
         double *p = io.dst + (long long)a * io.ds;
+        if (!io.tile && kp.out_mode != OUT_STORE) {
+#pragma unroll
+            for (int t = 0; t < M; ++t) {
+                double x = R.r[t] + Q1 * kp.ps[t];
+                if (ORDER2) x += Q2 * kp.pt[t];
+                if (HAS_DELTA) x *= de;
+                out_put(kp, p + (long long)t * io.ds, x);
+            }
+            return;
+        }
 #pragma unroll
         for (int t = 0; t < M; ++t) {
             double x = R.r[t] + Q1 * kp.ps[t];
@@ -684,6 +709,7 @@ struct LineKernel {
         if (!io.live) return;
         double *line = io.dst;
         const long long gs = io.ds;
+        const bool xf = !io.tile && kp.out_mode != OUT_STORE;
         if (fast(kp, s)) {
             fin_fast(kp, sm, R, l, s, io);
             return;
@@ -697,12 +723,18 @@ struct LineKernel {
                 double x = R.r[t] + Q1 * stt.x;
                 if (ORDER2) x += Q2 * stt.y;
                 if (HAS_DELTA) x = tld<STAGED>(tr + T_DELTA) * x;
-                line[(long long)(a + t) * gs] = x;
+                if (xf) out_put(kp, line + (long long)(a + t) * gs, x);
+                else line[(long long)(a + t) * gs] = x;
             }
         }
         if (CYC && s == kp.S - 1) {
-            line[(long long)nb * gs] = sm.eb[(size_t)l * 4 + 0];
-            if (kp.nbord == 2) line[(long long)(nb + 1) * gs] = sm.eb[(size_t)l * 4 + 1];
+            if (xf) {
+                out_put(kp, line + (long long)nb * gs, sm.eb[(size_t)l * 4 + 0]);
+                if (kp.nbord == 2) out_put(kp, line + (long long)(nb + 1) * gs, sm.eb[(size_t)l * 4 + 1]);
+            } else {
+                line[(long long)nb * gs] = sm.eb[(size_t)l * 4 + 0];
+                if (kp.nbord == 2) line[(long long)(nb + 1) * gs] = sm.eb[(size_t)l * 4 + 1];
+            }
         }
     }
 
@@ -779,6 +811,7 @@ PADO_HD PADO_INLINE LineIO tile_line_io(const KParams &kp, const Smem &sm, int l
     const bool out_tile = ADJ || IN == IN_LINES;
     io.dst = out_tile ? sm.tile + (size_t)l * kp.P : kp.out + base;
     io.ds = out_tile ? 1 : kp.stride;
+    io.tile = out_tile;
     return io;
 }
 
@@ -968,6 +1001,7 @@ __global__ void __launch_bounds__(M <= 8 ? 1024 : (M <= 32 ? 512 : 256), 1) line
         LineIO out = io;
         out.dst = kp.out + line_base(kp, io.live ? q0 + l : 0);
         out.ds = kp.stride;
+        out.tile = false;
         if (active) K::template fin<false>(kp, sm, R, l, s, out);
     }
 }

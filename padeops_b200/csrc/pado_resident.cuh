@@ -31,6 +31,18 @@
 
 namespace pado {
 
+// fin with the launch's output mode (scaled / accumulated results), defined
+// after ResidentLine
+template <int RK, bool PER, int M, bool ADJ, bool STAGED>
+#ifdef __CUDA_ARCH__
+__device__ __noinline__
+#else
+inline
+#endif
+    void
+    fin_out_mode(const KParams &kp, const Smem &sm, const double *line, long long rs, int l, int s, double *out,
+                 long long os);
+
 template <int RK, bool PER, int M, bool ADJ = false>
 struct ResidentLine {
     static constexpr bool CYC = PER;
@@ -367,7 +379,7 @@ struct ResidentLine {
 
     // constant-coefficient segment: corrected x -> out; RSP: the rows also
     // take the border unknowns' response E1 R1 + E2 R2
-    template <bool RSP>
+    template <bool RSP, bool XF>
     static PADO_HD PADO_INLINE void fin_fast(const KParams &kp, const Smem &sm, const double *p, long long rs, double *q,
                                              long long os, int a, double Q1, double Q2, double E1, double E2)
     {
@@ -387,16 +399,31 @@ struct ResidentLine {
                 if (ORDER2) x += E2 * rr[1];
             }
             if (HAS_DELTA) x *= kp.kc[6];
-            q[(long long)t * os] = x;
+            if (XF) out_put(kp, q + (long long)t * os, x);
+            else q[(long long)t * os] = x;
         }
     }
 
-    // ---- fin: corrected x -> out (row r at out[r * os]) ----------------------
+    // ---- fin: corrected x -> out (row r at out[r * os]); out_df: out is df
+    // itself, so the launch's output mode applies (else the tile).  The
+    // scaled / accumulating form runs out of line (fin_out_mode), so that the
+    // common form keeps its register allocation.
     template <bool STAGED>
     static PADO_HD PADO_INLINE void fin(const KParams &kp, const Smem &sm, const double *line, long long rs, int l,
-                                        int s, double *out, long long os, bool live)
+                                        int s, double *out, long long os, bool live, bool out_df = false)
     {
         if (!live) return;
+        if (out_df && kp.out_mode != OUT_STORE) {
+            fin_out_mode<RK, PER, M, ADJ, STAGED>(kp, sm, line, rs, l, s, out, os);
+            return;
+        }
+        fin_body<STAGED, false>(kp, sm, line, rs, l, s, out, os);
+    }
+
+    template <bool STAGED, bool XF>
+    static PADO_HD PADO_INLINE void fin_body(const KParams &kp, const Smem &sm, const double *line, long long rs, int l,
+                                             int s, double *out, long long os)
+    {
         const int nb = kp.nb;
         const int a = seg_start(kp, s), len = seg_len(kp, s);
         const int lenb = (a + len <= nb) ? len : nb - a;
@@ -412,8 +439,8 @@ struct ResidentLine {
             E2 = sm.eb[(size_t)l * 4 + 1];
         }
         if (fast(kp, s)) {
-            if (spike_rows) fin_fast<true>(kp, sm, p, rs, q, os, a, Q1, Q2, E1, E2);
-            else fin_fast<false>(kp, sm, p, rs, q, os, a, Q1, Q2, 0.0, 0.0);
+            if (spike_rows) fin_fast<true, XF>(kp, sm, p, rs, q, os, a, Q1, Q2, E1, E2);
+            else fin_fast<false, XF>(kp, sm, p, rs, q, os, a, Q1, Q2, 0.0, 0.0);
             return;
         }
         const double *tb = seg_etab(sm, s);
@@ -428,11 +455,17 @@ struct ResidentLine {
                 if (ORDER2) x += E2 * rr[1];
             }
             if (HAS_DELTA) x *= tld<STAGED>(tb + (size_t)t * E_NF + E_DELTA);
-            q[(long long)t * os] = x;
+            if (XF) out_put(kp, q + (long long)t * os, x);
+            else q[(long long)t * os] = x;
         }
         if (CYC && s == kp.S - 1) {
-            out[(long long)nb * os] = sm.eb[(size_t)l * 4 + 0];
-            if (kp.nbord == 2) out[(long long)(nb + 1) * os] = sm.eb[(size_t)l * 4 + 1];
+            if (XF) {
+                out_put(kp, out + (long long)nb * os, sm.eb[(size_t)l * 4 + 0]);
+                if (kp.nbord == 2) out_put(kp, out + (long long)(nb + 1) * os, sm.eb[(size_t)l * 4 + 1]);
+            } else {
+                out[(long long)nb * os] = sm.eb[(size_t)l * 4 + 0];
+                if (kp.nbord == 2) out[(long long)(nb + 1) * os] = sm.eb[(size_t)l * 4 + 1];
+            }
         }
     }
 
@@ -539,5 +572,18 @@ struct ResidentLine {
         }
     }
 };
+
+template <int RK, bool PER, int M, bool ADJ, bool STAGED>
+#ifdef __CUDA_ARCH__
+__device__ __noinline__
+#else
+inline
+#endif
+    void
+    fin_out_mode(const KParams &kp, const Smem &sm, const double *line, long long rs, int l, int s, double *out,
+                 long long os)
+{
+    ResidentLine<RK, PER, M, ADJ>::template fin_body<STAGED, true>(kp, sm, line, rs, l, s, out, os);
+}
 
 }  // namespace pado

@@ -336,10 +336,28 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
                 if (active) RL::adj_out(kp, line, rs, s, dst, XL ? 1 : io.ds, io.live);
             }
         } else {
-            if (active) RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live);
+            if (active) RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live, !XL);
         }
         const long long tn = t + (long long)stages * G;  // tile for this buffer next
         if (XL && (!ADJ || adj_tile)) {
+            if (!ADJ && kp.out_mode != OUT_STORE) {
+                // scaled or accumulated output: the tile's lines take df's values
+                // (contiguous, read by whole warps) before they go out
+                __syncthreads();
+                const long long nl_ = kp.nlines - x0;
+                const int nl = (int)(nl_ < L ? nl_ : L);
+                const int warp = tid >> 5, lane = tid & 31, nw = nthreads >> 5;
+                for (int ll = warp; ll < nl; ll += nw) {
+                    double *dl = kp.out + (x0 + ll) * (long long)kp.n;
+                    double *tl = sm.tile + (size_t)ll * kp.P;
+                    for (int r = lane; r < kp.n; r += 32) {
+                        double v = dl[r];
+                        if (kp.out_mode == OUT_ACC) v = fma(kp.out_alpha, tl[r], v);
+                        else v = kp.out_alpha * tl[r];
+                        tl[r] = v;
+                    }
+                }
+            }
             // each line's results -> global memory, then the buffer takes the next load
             fence_proxy_async();
             __syncthreads();
@@ -419,7 +437,7 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
                 case 2: RL::template bwd<true>(kp, sm, line, rs, l, s); break;
                 case 3:
                     if (ADJ) RL::template fin<true>(kp, sm, line, rs, l, s, line, rs, true);
-                    else RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live);
+                    else RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live, !XL);
                     break;
                 case 4:
                     if (adj_tile) RL::adj_gather(kp, line, rs, l, s, sm.buf4, H[tid]);
@@ -433,7 +451,11 @@ inline void emulate_stream(const StreamParams &sp, int nthreads)
         }
         if (XL && (!ADJ || adj_tile))
             for (int ll = 0; ll < nl; ++ll)
-                for (int r = 0; r < kp.n; ++r) kp.out[(x0 + ll) * kp.n + r] = sm.tile[(size_t)ll * kp.P + r];
+                for (int r = 0; r < kp.n; ++r) {
+                    double *d = kp.out + (x0 + ll) * kp.n + r;
+                    if (ADJ) *d = sm.tile[(size_t)ll * kp.P + r];
+                    else out_put(kp, d, sm.tile[(size_t)ll * kp.P + r]);
+                }
     }
 }
 

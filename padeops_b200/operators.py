@@ -131,16 +131,25 @@ class _Scheme:
 
     # -- generic apply ----------------------------------------------------------
     def apply(self, kind: int, axis: int, f: torch.Tensor, df: torch.Tensor, na: int, nb: int,
-              bc1: int | None = None, bcn: int | None = None, adjoint: bool = False) -> torch.Tensor:
+              bc1: int | None = None, bcn: int | None = None, adjoint: bool = False, alpha: float = 1.0,
+              beta: float = 0.0) -> torch.Tensor:
+        """df = alpha * D f + beta * df (beta 0 or 1; pado_apply_scaled), or
+        D^T f for ``adjoint`` (alpha 1, beta 0 only)."""
         numel = self.n * int(na) * int(nb)
         _check_field(f, numel, "f")
         _check_field(df, numel, "df")
         if f.device != df.device:
             raise ValueError("f and df must be on the same device")
-        fn = L.lib().pado_apply_adjoint if adjoint else L.lib().pado_apply
+        b1, bn = 0 if bc1 is None else int(bc1), 0 if bcn is None else int(bcn)
         with torch.cuda.device(f.device):
-            st = fn(self.handle, kind, axis, f.data_ptr(), df.data_ptr(), int(na), int(nb),
-                    0 if bc1 is None else int(bc1), 0 if bcn is None else int(bcn), _stream_ptr(f))
+            if alpha != 1.0 or beta != 0.0:
+                if adjoint:
+                    raise PadoError(L.E_UNSUPPORTED, "the adjoint has no scaled or accumulating form")
+                st = L.lib().pado_apply_scaled(self.handle, kind, axis, f.data_ptr(), df.data_ptr(), int(na), int(nb),
+                                               b1, bn, float(alpha), float(beta), _stream_ptr(f))
+            else:
+                fn = L.lib().pado_apply_adjoint if adjoint else L.lib().pado_apply
+                st = fn(self.handle, kind, axis, f.data_ptr(), df.data_ptr(), int(na), int(nb), b1, bn, _stream_ptr(f))
         check(st, f"{type(self).__name__}.{'adjoint' if adjoint else 'apply'}(kind={kind}, axis={axis})")
         return df
 
@@ -291,7 +300,7 @@ class Derivatives:
         nx, ny, nz = self.sz
         return {1: (ny, nz), 2: (nx, nz), 3: (nx, ny)}[axis]
 
-    def _d(self, kind, axis, f, df, bc1, bcn):
+    def _d(self, kind, axis, f, df, bc1, bcn, alpha=1.0, beta=0.0):
         op = self.ops[axis - 1]
         if kind == L.D2 and isinstance(op, cd06):
             raise PadoError(L.E_UNSUPPORTED, "cd06 has no second derivative (derivatives.F90:525)")
@@ -300,7 +309,12 @@ class Derivatives:
             bc1 = bcn = None
         elif bc1 is None or bcn is None:  # the bc pair is forwarded only when both are present
             bc1 = bcn = None
-        return op.apply(kind, axis, f, df, na, nb, bc1, bcn)
+        return op.apply(kind, axis, f, df, na, nb, bc1, bcn, alpha=alpha, beta=beta)
+
+    def apply(self, kind, axis, f, df, bc1=None, bcn=None, alpha=1.0, beta=0.0):
+        """df = alpha * D f + beta * df along ``axis`` (1 x, 2 y, 3 z), D the first
+        (kind 1) or second (kind 2) derivative of that direction's scheme."""
+        return self._d(kind, axis, f, df, bc1, bcn, alpha, beta)
 
     def ddx(self, f, df, bc1=None, bcn=None):
         return self._d(L.D1, 1, f, df, bc1, bcn)
