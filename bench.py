@@ -90,23 +90,28 @@ class ClockSampler:
         self.samples: list[tuple[float, float, set]] = []
 
     def _nvml_handle(self):
+        """NVML handle of CUDA device `index`, found by its PCI bus id; returns
+        (module, handle, bus id).  Without the bus id the NVML index is used
+        only when CUDA_VISIBLE_DEVICES does not renumber the devices."""
         import pynvml
         import torch
 
         pynvml.nvmlInit()
+        bus = None
         try:
             prop = torch.cuda.get_device_properties(self.index)
             bus = f"{prop.pci_domain_id:08x}:{prop.pci_bus_id:02x}:{prop.pci_device_id:02x}.0"
-            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus), bus
         except Exception:
-            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            if os.environ.get("CUDA_VISIBLE_DEVICES"):
+                raise
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index), bus
 
-    def _poll(self, nv, h):
+    def _poll(self, nv, h, mx):
         bits = [getattr(nv, "nvmlClocksEventReason" + k, getattr(nv, "nvmlClocksThrottleReason" + k, 0))
                 for k in ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
         reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
                              getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
-        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         while not self.stop.is_set():
             try:
                 sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
@@ -117,16 +122,26 @@ class ClockSampler:
             time.sleep(0.01)
 
     def __enter__(self):
+        self.bus = None
         try:
-            nv, h = self._nvml_handle()
+            nv, h, self.bus = self._nvml_handle()
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))  # fails here, not in the thread
             self.nvml = nv
-            self.t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.t = threading.Thread(target=self._poll, args=(nv, h, mx), daemon=True)
             self.t.start()
             return self
         except Exception:
+            if self.nvml is None:
+                try:
+                    import pynvml
+
+                    pynvml.nvmlShutdown()
+                except Exception:
+                    pass
             self.nvml = None
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+            dev = self.bus if self.bus else str(self.index)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", dev, f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -178,7 +193,8 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi",
+                "pci_bus_id": self.bus}
 
 
 def make_field(seed: int) -> np.ndarray:
@@ -187,28 +203,49 @@ def make_field(seed: int) -> np.ndarray:
     return spectrum53((N, N, N), seed)
 
 
-def cpu_baseline(f: np.ndarray, threads: int, budget_s: float = 20.0) -> dict:
-    """Times the oracle built with the reference's Release flags on the host cores."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def _cpu_rate(f: np.ndarray, threads: int, budget_s: float, max_ops: int = 9) -> tuple[float, int]:
+    """Gpts/s of the oracle (the reference's Release flags) over the step's
+    operator applications, as many as fit the budget (at least one)."""
     import oracle
 
     dx = 2 * np.pi / N
     ops = [oracle.OracleOp({"cd10": oracle.CD10, "cf90": oracle.CF90}[s], N, dx, True, fast=True) for s, _ in OPS]
     out = np.empty_like(f)
-    pts = 0
     t0 = time.perf_counter()
     done = []
-    while time.perf_counter() - t0 < budget_s and len(done) < 9:
+    while len(done) < max_ops and (not done or time.perf_counter() - t0 < budget_s):
         i = len(done)
         op, (s, kind) = ops[i % 3], OPS[i % 3]
         axis = i // 3 + 1
         ts = time.perf_counter()
         op.apply(kind, axis, f, N, N, 0, 0, nthreads=threads, out=out)
         done.append(time.perf_counter() - ts)
-        pts += N ** 3
-    el = sum(done)
-    return {"value": pts / el / 1e9, "unit": "Gpts/s", "cores": threads, "kind": "port",
-            "sample": f"{len(done)} of the 9 operator applications on the 512^3 field "
-                      f"(oracle, -O3 -ffast-math -march=x86-64-v3, OpenMP {threads} threads)"}
+    return len(done) * N ** 3 / sum(done) / 1e9, len(done)
+
+
+def cpu_baseline(f: np.ndarray, threads: int, budget_s: float = 20.0) -> dict:
+    """The oracle built with the reference's Release flags on the host cores:
+    all cores (OpenMP over independent lines, a stand-in for the reference's
+    MPI ranks) and one thread (the reference's per-rank behaviour: its
+    compact-scheme modules have no OpenMP)."""
+    v_all, n_all = _cpu_rate(f, threads, budget_s)
+    v_one, n_one = _cpu_rate(f, 1, budget_s / 2, max_ops=1)
+    return {"value": v_all, "unit": "Gpts/s", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
+            "threads_all": {"value": v_all, "threads": threads, "applications": n_all},
+            "threads_1": {"value": v_one, "threads": 1, "applications": n_one},
+            "sample": f"{n_all} of the 9 operator applications on the 512^3 field with {threads} threads, "
+                      f"{n_one} with 1 thread (oracle, -O3 -ffast-math -march=x86-64-v3, OpenMP)"}
 
 
 def run_reference(args) -> None:
@@ -299,7 +336,59 @@ def extensions() -> dict:
     adj_ms = ev_ms(lambda: (dx_op.apply(1, 1, u, o1, n, n, adjoint=True), dz_op.apply(1, 3, u, o2, n, n, adjoint=True)))
     adjoint = {"workload": "D_x^cd10 (periodic) + D_z^cd06 (bounded) on 256^3", "fwd_ms": round(fwd_ms, 4),
                "adjoint_ms": round(adj_ms, 4), "adjoint_over_forward": round(adj_ms / fwd_ms, 3)}
-    return {"batched": batched, "adjoint": adjoint}
+    del u, o1, o2
+    torch.cuda.empty_cache()
+    return {"batched": batched, "adjoint": adjoint, "field_ops": field_operators(ev_ms, gen)}
+
+
+def field_operators(ev_ms, gen) -> dict:
+    """The field operators of operators.F90 / cgrid%laplacian on 512^3 (cd10
+    periodic x, y; cd10 bounded z), each term summed into its output inside
+    the kernels.  Algorithmic bytes per output point: a stored term 16 (read
+    f, write df), an accumulated term 24 (read f, read and write df), so
+    gradient 3 x 16 (three outputs), laplacian and divergence 16 + 24 + 24,
+    curl 3 x (16 + 24).  Plus the laplacian of a pinned host field through
+    pado_apply_host_terms (one upload, one download)."""
+    import torch
+
+    import padeops_b200 as pb
+    from padeops_b200 import field_ops
+
+    n = N
+    dx, dz = 2 * np.pi / n, 1.0 / (n - 1)
+    der = pb.Derivatives()
+    der.init(n, n, n, dx, dx, dz, True, True, False, "cd10", "cd10", "cd10")
+    u, v, w = (torch.randn((n, n, n), dtype=torch.float64, device="cuda", generator=gen) for _ in range(3))
+    o = [torch.empty_like(u) for _ in range(3)]
+    cu = torch.stack(o)  # (3, n, n, n)
+    del o
+    pts = n ** 3
+    cases = {
+        "gradient": (lambda: field_ops.gradient(der, u, cu[0], cu[1], cu[2]), 3 * pts, 48),
+        "laplacian": (lambda: field_ops.laplacian(der, u, cu[0]), pts, 64),
+        "divergence": (lambda: field_ops.divergence(der, u, v, w, cu[0]), pts, 64),
+        "curl": (lambda: field_ops.curl(der, u, v, w, cu), 3 * pts, 120),
+    }
+    out = {"workload": "cd10 periodic x/y, cd10 bounded z, 512^3 FP64"}
+    for name, (fn, out_pts, bpt) in cases.items():
+        ms = ev_ms(fn)
+        out[name] = {"ms": round(ms, 3), "bytes_per_point": bpt, "gbs": round(pts * bpt / (ms / 1e3) / 1e9, 1),
+                     "gpts_out": round(out_pts / ms / 1e6, 1)}
+    hf = u.cpu().pin_memory()
+    hl = torch.empty_like(hf).pin_memory()
+    field_ops.laplacian_host(der, hf, hl)
+    t0 = time.perf_counter()
+    reps = 2
+    for _ in range(reps):
+        field_ops.laplacian_host(der, hf, hl)
+    el = (time.perf_counter() - t0) / reps
+    out["laplacian_host"] = {"ms": round(el * 1e3, 2), "gpts": round(pts / el / 1e9, 2),
+                             "h2d_bytes": pts * 8, "d2h_bytes": pts * 8,
+                             "path": "pado_apply_host_terms (pinned): one upload, 3 terms, one download"}
+    del u, v, w, cu, hf, hl
+    der.destroy()
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_gpu(args) -> None:

@@ -145,6 +145,27 @@ int pado_filter3_complex(pado_op_t op, const double *f, double *df, long na, lon
 int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, double *df_host, long na, long nb,
                     int bc1, int bcn, void *stream);
 
+/* One term of a host-buffer field operator: output[out] = alpha * D f +
+ * beta * output[out], D = op's (kind, axis, bc1, bcn) operator. */
+typedef struct {
+    pado_op_t op;
+    int kind, axis, bc1, bcn;
+    double alpha, beta; /* beta 0 or 1; the first term of an output has beta 0 */
+    int out;            /* output index; each output's terms are consecutive, outputs in order */
+} pado_host_term;
+
+/* Several operators on one host field f(n1,n2,n3), uploading f once: the
+ * host-buffer form of gradient (3 outputs, 1 term each), laplacian (1 output,
+ * 3 terms summed in the kernels) or any list of terms.  Each output is copied
+ * back while the next one is computed; two output fields and f are staged on
+ * the device (through terms[0].op's staging buffers and copy streams).
+ * Returns when every out_host[k] holds its result.  PADO_E_ARG for terms out
+ * of order, a first term with beta != 0 or an op whose n is not the extent
+ * along its axis.  No counterpart in the reference, whose solver holds its
+ * fields on the host and calls dd* per direction. */
+int pado_apply_host_terms(const double *f_host, long n1, long n2, long n3, const pado_host_term *terms, int nterms,
+                          double *const *out_host, int nout, void *stream);
+
 /* ---- tuning ------------------------------------------------------------- */
 
 /* Launch shape of the line kernels for this handle: m = segment length

@@ -35,6 +35,11 @@ class BatchItem(ctypes.Structure):
                 ("f", ctypes.c_void_p), ("df", ctypes.c_void_p)]
 
 
+class HostTerm(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_void_p), ("kind", ctypes.c_int), ("axis", ctypes.c_int), ("bc1", ctypes.c_int),
+                ("bcn", ctypes.c_int), ("alpha", ctypes.c_double), ("beta", ctypes.c_double), ("out", ctypes.c_int)]
+
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -54,6 +59,7 @@ SIGNATURES = {
     "pado_apply_adjoint": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, _P]),
     "pado_apply_scaled": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, _D, _D, _P]),
     "pado_apply_host": (_I, [_P, _I, _I, _P, _P, _L, _L, _I, _I, _P]),
+    "pado_apply_host_terms": (_I, [_P, _L, _L, _L, ctypes.POINTER(HostTerm), _I, ctypes.POINTER(_P), _I, _P]),
     "pado_set_tiling": (_I, [_P, _I, _I]),
     "pado_set_kernel_variant": (_I, [_P, _I]),
     "pado_device_status": (_I, [_P, _I]),

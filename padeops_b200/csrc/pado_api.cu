@@ -670,6 +670,93 @@ int pado_apply_host(pado_op_t op, int kind, int axis, const double *f_host, doub
     return e3 == cudaSuccess ? PADO_OK : cuda_fail(e3);
 }
 
+int pado_apply_host_terms(const double *f_host, long n1, long n2, long n3, const pado_host_term *terms, int nterms,
+                          double *const *out_host, int nout, void *stream)
+{
+    if (!f_host || !terms || !out_host) return PADO_E_NULL;
+    if (n1 < 1 || n2 < 1 || n3 < 1 || nterms < 1 || nout < 1) return PADO_E_ARG;
+    const long ext[3] = {n1, n2, n3};
+    for (int i = 0; i < nterms; ++i) {
+        const pado_host_term &t = terms[i];
+        if (!t.op) return PADO_E_NULL;
+        if (t.axis < 1 || t.axis > 3 || t.op->n != ext[t.axis - 1]) return PADO_E_ARG;
+        if (t.beta != 0.0 && t.beta != 1.0) return PADO_E_ARG;
+        const int prev = i ? terms[i - 1].out : -1;
+        if (t.out != prev && t.out != prev + 1) return PADO_E_ARG;  // outputs in order, terms consecutive
+        if (t.out != prev && t.beta != 0.0) return PADO_E_ARG;      // an output starts from its first term
+        if (t.out >= nout || !out_host[t.out]) return PADO_E_ARG;
+    }
+    if (terms[nterms - 1].out != nout - 1) return PADO_E_ARG;
+    pado_op_s *op0 = terms[0].op;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> g(op0->staging_mu);
+    const size_t total = (size_t)n1 * (size_t)n2 * (size_t)n3;
+    const size_t slot = (total + 31) / 32 * 32;
+    // f in stage_f, two output fields in stage_df
+    if (op0->stage_elems < 2 * slot) {
+        if (op0->stage_f) cudaFree(op0->stage_f);
+        if (op0->stage_df) cudaFree(op0->stage_df);
+        op0->stage_f = op0->stage_df = nullptr;
+        op0->stage_elems = 0;
+        cudaError_t e = cudaMalloc(&op0->stage_f, 2 * slot * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&op0->stage_df, 2 * slot * sizeof(double));
+        if (e != cudaSuccess) return cuda_fail(e);
+        op0->stage_elems = 2 * slot;
+    }
+    if (!op0->s_h2d) {
+        cudaError_t e = cudaStreamCreateWithFlags(&op0->s_h2d, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&op0->s_d2h, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(e);
+    }
+    // events: [0] f arrived, then per output: computed, copied out
+    const size_t nev = 1 + 2 * (size_t)nout;
+    while (op0->ev_in.size() < nev) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        cudaError_t e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e);
+        op0->ev_in.push_back(a);
+        op0->ev_out.push_back(b);
+    }
+    const size_t chunk = HOST_CHUNK_BYTES * 4 / sizeof(double);
+    int rc = PADO_OK;
+    cudaError_t e = cudaSuccess;
+    for (size_t o = 0; o < total && e == cudaSuccess; o += chunk)
+        e = cudaMemcpyAsync(op0->stage_f + o, f_host + o, std::min(chunk, total - o) * sizeof(double),
+                            cudaMemcpyHostToDevice, op0->s_h2d);
+    if (e == cudaSuccess) e = cudaEventRecord(op0->ev_in[0], op0->s_h2d);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, op0->ev_in[0], 0);
+    int i = 0;
+    for (int o = 0; o < nout && e == cudaSuccess && rc == PADO_OK; ++o) {
+        double *dev = op0->stage_df + (size_t)(o & 1) * slot;
+        // the buffer's previous output has left the device
+        if (o >= 2) e = cudaStreamWaitEvent(st, op0->ev_out[1 + 2 * (o - 2) + 1], 0);
+        for (; e == cudaSuccess && rc == PADO_OK && i < nterms && terms[i].out == o; ++i) {
+            const pado_host_term &t = terms[i];
+            const long na = t.axis == 1 ? n2 : n1, nb = t.axis == 3 ? n2 : n3;
+            const int mode = t.beta == 1.0 ? OUT_ACC : (t.alpha == 1.0 ? OUT_STORE : OUT_SCALE);
+            rc = launch(t.op, t.kind, t.axis, op0->stage_f, dev, na, nb, t.bc1, t.bcn, st, false, SAME_BC, SAME_BC,
+                        mode, t.alpha);
+        }
+        if (rc != PADO_OK || e != cudaSuccess) break;
+        e = cudaEventRecord(op0->ev_out[1 + 2 * o], st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(op0->s_d2h, op0->ev_out[1 + 2 * o], 0);
+        for (size_t c = 0; c < total && e == cudaSuccess; c += chunk)
+            e = cudaMemcpyAsync(out_host[o] + c, dev + c, std::min(chunk, total - c) * sizeof(double),
+                                cudaMemcpyDeviceToHost, op0->s_d2h);
+        if (e == cudaSuccess) e = cudaEventRecord(op0->ev_out[1 + 2 * o + 1], op0->s_d2h);
+    }
+    // every copy that was enqueued ends before the host buffers are handed back
+    const cudaError_t e1 = cudaStreamSynchronize(op0->s_h2d);
+    const cudaError_t e2 = cudaStreamSynchronize(op0->s_d2h);
+    const cudaError_t e3 = cudaStreamSynchronize(st);
+    if (rc != PADO_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (e1 != cudaSuccess) return cuda_fail(e1);
+    if (e2 != cudaSuccess) return cuda_fail(e2);
+    return e3 == cudaSuccess ? PADO_OK : cuda_fail(e3);
+}
+
 int pado_set_tiling(pado_op_t op, int m, int lines)
 {
     if (!op) return PADO_E_NULL;

@@ -28,7 +28,8 @@ import torch
 
 from . import _lib as L
 
-__all__ = ["gradient", "curl", "divergence", "laplacian", "filter3d"]
+__all__ = ["gradient", "curl", "divergence", "laplacian", "filter3d", "apply_host_terms", "gradient_host",
+           "laplacian_host"]
 
 _BC0 = (0, 0)
 
@@ -88,3 +89,47 @@ def filter3d(fil, arr: torch.Tensor, numtimes: int = 1, x_bc=_BC0, y_bc=_BC0, z_
     if a.data_ptr() != arr.data_ptr():
         arr.copy_(a)
     return arr
+
+
+def _host_ptr(a) -> int:
+    import numpy as np
+
+    if isinstance(a, torch.Tensor):
+        if a.is_cuda or a.dtype != torch.float64 or not a.is_contiguous():
+            raise ValueError("host fields must be contiguous float64 CPU arrays")
+        return a.data_ptr()
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+        raise ValueError("host fields must be contiguous float64 CPU arrays")
+    return a.ctypes.data
+
+
+def apply_host_terms(f, shape, terms, outs) -> None:
+    """Host-buffer field operator (pado_apply_host_terms): f uploaded once, then
+    every term (op, kind, axis, bc1, bcn, alpha, beta, out) applied into
+    outs[out] on the device; each output is copied back while the next is
+    computed.  shape = (n3, n2, n1) of the column-major field."""
+    import ctypes
+
+    n3, n2, n1 = (int(v) for v in shape)
+    arr = (L.HostTerm * len(terms))()
+    for i, (op, kind, axis, bc1, bcn, alpha, beta, out) in enumerate(terms):
+        arr[i] = L.HostTerm(op.handle, kind, axis, bc1, bcn, alpha, beta, out)
+    ptrs = (ctypes.c_void_p * len(outs))(*[_host_ptr(o) for o in outs])
+    st = L.lib().pado_apply_host_terms(_host_ptr(f), n1, n2, n3, arr, len(terms), ptrs, len(outs),
+                                      torch.cuda.current_stream().cuda_stream)
+    L.check(st, "apply_host_terms")
+
+
+def gradient_host(der, f, dfdx, dfdy, dfdz, x_bc=_BC0, y_bc=_BC0, z_bc=_BC0) -> None:
+    """gradient of a host field: one upload, three results copied back."""
+    ops = der.ops
+    apply_host_terms(f, f.shape, [(ops[1], L.D1, 2, *y_bc, 1.0, 0.0, 0), (ops[0], L.D1, 1, *x_bc, 1.0, 0.0, 1),
+                                  (ops[2], L.D1, 3, *z_bc, 1.0, 0.0, 2)], [dfdy, dfdx, dfdz])
+
+
+def laplacian_host(der, f, lapf, x_bc=_BC0, y_bc=_BC0, z_bc=_BC0) -> None:
+    """laplacian of a host field: one upload, the three terms summed on the
+    device, one result copied back."""
+    ops = der.ops
+    apply_host_terms(f, f.shape, [(ops[1], L.D2, 2, *y_bc, 1.0, 0.0, 0), (ops[0], L.D2, 1, *x_bc, 1.0, 1.0, 0),
+                                  (ops[2], L.D2, 3, *z_bc, 1.0, 1.0, 0)], [lapf])

@@ -112,3 +112,36 @@ def test_laplacian_and_divergence_full_field(torch_cuda):
     ref = od(oracle.D1, 2, v) + od(oracle.D1, 1, u)
     ref = ref + od(oracle.D1, 3, w, (-1, 1))
     assert rel_err(div.cpu().numpy(), ref) <= TOL
+
+
+def test_host_terms(torch_cuda):
+    """pado_apply_host_terms: gradient and laplacian of a host field (pinned and
+    pageable) equal the device-resident field operators bit for bit; terms out
+    of order are refused."""
+    import padeops_b200 as pb
+    from padeops_b200 import _lib as L
+    from padeops_b200 import field_ops
+
+    torch = torch_cuda
+    n1, n2, n3 = 96, 80, 64
+    shape = (n3, n2, n1)
+    f = spectrum53(shape, seed=9)
+    der = pb.Derivatives()
+    der.init(n1, n2, n3, 2 * np.pi / n1, 2 * np.pi / n2, 1.0 / (n3 - 1), True, True, False, "cd10", "cd10", "cd10")
+    ft = torch.from_numpy(f).cuda()
+    g = [torch.empty_like(ft) for _ in range(3)]
+    field_ops.gradient(der, ft, *g, z_bc=(1, -1))
+    lap = torch.empty_like(ft)
+    field_ops.laplacian(der, ft, lap, z_bc=(1, -1))
+    torch.cuda.synchronize()
+    for pinned in (True, False):
+        src = torch.from_numpy(f).pin_memory() if pinned else f
+        outs = [np.full(shape, np.nan) for _ in range(3)]
+        field_ops.gradient_host(der, src, *outs, z_bc=(1, -1))
+        for o, ref in zip(outs, g):
+            assert np.array_equal(o, ref.cpu().numpy())
+        lo = np.full(shape, np.nan)
+        field_ops.laplacian_host(der, src, lo, z_bc=(1, -1))
+        assert np.array_equal(lo, lap.cpu().numpy())
+    with pytest.raises(pb.PadoError):
+        field_ops.apply_host_terms(f, shape, [(der.ops[0], L.D1, 1, 0, 0, 1.0, 1.0, 0)], [np.empty(shape)])
