@@ -496,6 +496,79 @@ def run_gpu(args) -> None:
         dist.destroy_process_group()
 
 
+def run_configs(args) -> None:
+    """The per-config table of the benchmark's configurations on one GPU and
+    the host cores: C1 (cd06 periodic d1 on 64^3, 8 seeded sinusoids), C2
+    (cd10 d1, cd10 d2, cf90 periodic on 512^3), C3 (1024x512x256: cd06 and
+    cd10 d1 bounded along z, cd06 and cd10 d1 periodic along x and y).  GPU:
+    CUDA events over 20 applications after warm-up, per operator; CPU: the
+    oracle with the reference's Release flags, 1 thread and all host threads,
+    one application per operator.  Prints one JSON line."""
+    import torch
+
+    import oracle
+    import padeops_b200 as pb
+    from tests.fields import poly_z, sinusoids, spectrum53
+
+    threads = os.cpu_count() or 1
+    peak, _ = measured_peaks()
+    cls = {"cd06": (pb.cd06, oracle.CD06), "cd10": (pb.cd10, oracle.CD10), "cf90": (pb.cf90, oracle.CF90)}
+    rows = []
+
+    def measure(cfg, f_host, scheme, kind, axis, periodic, d):
+        shape = f_host.shape
+        n = shape[3 - axis]
+        na, nb = {1: (shape[1], shape[0]), 2: (shape[2], shape[0]), 3: (shape[2], shape[1])}[axis]
+        pcls, oscheme = cls[scheme]
+        op = pcls()
+        assert (op.init(n, periodic) if scheme == "cf90" else op.init(n, d, periodic, 0, 0)) == 0
+        f = torch.from_numpy(f_host).cuda()
+        df = torch.empty_like(f)
+        for _ in range(3):
+            op.apply(kind, axis, f, df, na, nb)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(20):
+            op.apply(kind, axis, f, df, na, nb)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 20
+        got = df.cpu().numpy()
+        o = oracle.OracleOp(oscheme, n, d if scheme != "cf90" else 1.0, periodic, fast=True)
+        cpu = {}
+        for t in (1, threads):
+            ts = time.perf_counter()
+            ref = o.apply(kind, axis, f_host, na, nb, nthreads=t)
+            cpu[t] = f_host.size / (time.perf_counter() - ts) / 1e9
+        strict = oracle.OracleOp(oscheme, n, d if scheme != "cf90" else 1.0, periodic).apply(
+            kind, axis, f_host, na, nb, nthreads=threads).reshape(shape)
+        err = float(np.abs(got - strict).max() / np.abs(strict).max())
+        gpts = f_host.size / ms / 1e6
+        rows.append({"config": cfg, "op": f"{scheme} {'d1' if kind == 1 else 'd2' if kind == 2 else 'filter'}",
+                     "axis": axis, "periodic": periodic, "shape": list(shape)[::-1], "gpu_us": round(ms * 1e3, 1),
+                     "gpu_gpts": round(gpts, 1), "hbm_frac": round(gpts * 16 / peak, 3),
+                     "cpu_1thr_gpts": round(cpu[1], 3), "cpu_all_gpts": round(cpu[threads], 3),
+                     "max_rel_err_vs_oracle": err})
+        del f, df
+
+    f1 = sinusoids(64, seed=1)
+    for axis in (1, 2, 3):
+        measure("C1", f1, "cd06", 1, axis, True, 2 * np.pi / 64)
+    f2 = spectrum53((N, N, N), seed=7)
+    for scheme, kind in OPS:
+        for axis in (1, 2, 3):
+            measure("C2", f2, scheme, kind, axis, True, 2 * np.pi / N)
+    del f2
+    f3 = poly_z((256, 512, 1024), seed=3)
+    for scheme in ("cd06", "cd10"):
+        measure("C3", f3, scheme, 1, 3, False, 1.0 / 255)
+        measure("C3", f3, scheme, 1, 1, True, 2 * np.pi / 1024)
+        measure("C3", f3, scheme, 1, 2, True, 2 * np.pi / 512)
+    print(json.dumps({"configs": rows, "cpu_model": cpu_model(), "cpu_threads": threads, "hbm_peak_gbs": peak}),
+          flush=True)
+
+
 def run_single_op(args) -> None:
     """One operator on one field, a few times: the small cases the ncu summaries
     under profiles/ are captured on (prints the launch plan)."""
@@ -569,8 +642,11 @@ def main() -> None:
     ap.add_argument("--bounded", action="store_true", help="profiling: bounded instead of periodic lines")
     ap.add_argument("--repeat", type=int, default=3, help="profiling: applications of the operator")
     ap.add_argument("--adjoint", action="store_true", help="profiling: the adjoint operator")
+    ap.add_argument("--configs", action="store_true", help="the per-config table (C1-C3, GPU and CPU)")
     args = ap.parse_args()
-    if args.op:
+    if args.configs:
+        run_configs(args)
+    elif args.op:
         run_single_op(args)
     elif args.impl == "reference":
         run_reference(args)
