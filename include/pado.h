@@ -270,7 +270,9 @@ void pado_batch_destroy(pado_batch_t batch);
  *     that device current); make it before any stream capture.
  *   - All calls on a device share the one array: two calls whose launches
  *     overlap on the GPU race and give wrong results.  Order them on one
- *     stream, or wait for one before starting the next.
+ *     stream, or wait for one before starting the next.  Calls made from
+ *     several host threads at once are serialized inside the library, so
+ *     their copies and launches do not interleave on a shared stream.
  *   - Every item's operator must belong to the current device.
  * No counterpart in the reference. */
 int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream);

@@ -439,6 +439,9 @@ constexpr int STATIC_CHUNK = 8;      // descriptors staged per host-to-device co
 
 std::mutex g_static_mu;
 unsigned char *g_static_addr[STATIC_MAX_DEVICES] = {};
+// held through a whole pado_batch_run_static call, so that calls from several
+// host threads enqueue their copies and launch one after the other
+std::mutex g_static_run_mu;
 
 }  // namespace
 
@@ -476,6 +479,7 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
     unsigned char *base = nullptr;
     int rc = static_scratch(dev, &base);
     if (rc != PADO_OK) return rc;
+    std::lock_guard<std::mutex> run_lock(g_static_run_mu);
 
     // pass 1: validate, cost and tile count of every item (no descriptor kept)
     double cost[PADO_STATIC_BATCH_MAX_ITEMS];

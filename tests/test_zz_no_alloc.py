@@ -76,6 +76,32 @@ def test_static_batch_matches_apply_on_two_calls():
     _check_against_apply(torch, second)
 
 
+def test_static_batch_allocates_nothing_and_calls_back_to_back():
+    """Two calls in a row on one stream with no synchronization between them
+    (the second call's descriptor copies wait behind the first launch on the
+    stream), then both outputs against pado_apply; device memory in use --
+    the driver's count and torch's -- is the same before and after."""
+    import torch
+
+    first = _workload(torch, 31, seed=4)
+    second = _workload(torch, 17, seed=5)
+    assert _run_static(torch, first) == 0  # the first call on this device sets up the scratch address
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for it in first + second:
+        it[4].fill_(float("nan"))
+    torch.cuda.synchronize()
+    assert _run_static(torch, first) == 0
+    assert _run_static(torch, second) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert torch.cuda.memory_allocated() == alloc0
+    assert free1 == free0
+    _check_against_apply(torch, first)
+    _check_against_apply(torch, second)
+
+
 def test_static_batch_rejects_too_many_items():
     import torch
 
