@@ -277,6 +277,50 @@ void pado_batch_destroy(pado_batch_t batch);
  * No counterpart in the reference. */
 int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream);
 
+/* ---- staggered sixth-order compact scheme (cd06stagg, along z) ---------- */
+
+/* cd06staggstuff (src/derivatives/cd06stagg.F90): first derivatives
+ * edge->cell, cell->edge, cell->cell and edge->edge, second derivatives
+ * cell->cell and edge->edge, and interpolation edge->cell and cell->edge,
+ * along the third index of (n1, n2, nz) column-major fields.  The cell grid
+ * has n points, the edge grid n + 1.  Used by the incompressible solver
+ * (src/incompressible/PadeDerOps.F90). */
+typedef struct pado_stagg_s *pado_stagg_t;
+
+/* Operators, the reference's procedure names in order
+ * (ddz_E2C .. InterpZ_C2E, cd06stagg.F90:820-1060). */
+#define PADO_STAGG_DDZ_E2C 0
+#define PADO_STAGG_DDZ_C2E 1
+#define PADO_STAGG_DDZ_C2C 2
+#define PADO_STAGG_DDZ_E2E 3
+#define PADO_STAGG_D2DZ2_C2C 4
+#define PADO_STAGG_D2DZ2_E2E 5
+#define PADO_STAGG_INTERPZ_E2C 6
+#define PADO_STAGG_INTERPZ_C2E 7
+#define PADO_STAGG_NOPS 8
+/* nx <= 4: the reference stops with GracefulExit(..., 21) (cd06stagg.F90:183-185). */
+#define PADO_STAGG_E_SHORT 21
+
+/* cd06stagg%init_periodic(nx, dx) (cd06stagg.F90:170-195). */
+int pado_cd06stagg_init_periodic(pado_stagg_t *stagg, int nx, double dx);
+/* cd06stagg%init_nonperiodic(nx, dx, isTopEven, isBotEven, isTopSided,
+ * isBotSided) (cd06stagg.F90:197-232); the sided flags are 0 when the
+ * reference's optional arguments are absent. */
+int pado_cd06stagg_init_nonperiodic(pado_stagg_t *stagg, int nx, double dx, int is_top_even, int is_bot_even,
+                                    int is_top_sided, int is_bot_sided);
+/* Planes along z read (nin) and written (nout) by operator `op`: n or n + 1.
+ * PADO_E_UNSUPPORTED for the C2C / E2E first derivatives of a periodic
+ * object (the reference solves them with tables its periodic init never
+ * allocates). */
+int pado_cd06stagg_sizes(pado_stagg_t stagg, int op, int *nin, int *nout);
+/* df(n1, n2, nout) = op applied along z to f(n1, n2, nin): device pointers,
+ * enqueued on `stream`; f and df must not overlap.  A complex field is
+ * passed as its (re, im) doubles with n1 doubled (the coefficients are
+ * real). */
+int pado_cd06stagg_apply(pado_stagg_t stagg, int op, const double *f, double *df, long n1, long n2, void *stream);
+/* cd06stagg%destroy (cd06stagg.F90:234-243). */
+void pado_cd06stagg_destroy(pado_stagg_t stagg);
+
 /* ---- diagnostics -------------------------------------------------------- */
 
 const char *pado_strerror(int status);

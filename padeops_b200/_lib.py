@@ -77,6 +77,11 @@ SIGNATURES = {
     "pado_batch_run_static": (_I, [_P, _I, _P]),
     "pado_batch_set_graph_branches": (_I, [_P, _I]),
     "pado_filter3_complex": (_I, [_P, _P, _P, _L, _L, _I, _I, _P]),
+    "pado_cd06stagg_init_periodic": (_I, [ctypes.POINTER(_P), _I, _D]),
+    "pado_cd06stagg_init_nonperiodic": (_I, [ctypes.POINTER(_P), _I, _D, _I, _I, _I, _I]),
+    "pado_cd06stagg_sizes": (_I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "pado_cd06stagg_apply": (_I, [_P, _I, _P, _P, _L, _L, _P]),
+    "pado_cd06stagg_destroy": (None, [_P]),
     "pado_strerror": (ctypes.c_char_p, [_I]),
     "pado_launch_count": (ctypes.c_longlong, []),
     "pado_version": (ctypes.c_char_p, []),

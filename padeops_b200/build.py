@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpado.so")
-SOURCES = ["pado_api.cu", "pado_batch.cu", "pado_tables.cpp", "pado_inst.cu"]
+SOURCES = ["pado_api.cu", "pado_batch.cu", "pado_tables.cpp", "pado_inst.cu", "pado_stagg.cu"]
 HEADERS = ["pado_common.h", "pado_tables.h", "pado_kernels.cuh", "pado_batch.cuh", "pado_internal.h", "pado_params.h",
            "pado_stream.cuh", "pado_resident.cuh"]
 # pado_inst.cu is compiled once per stencil (-DPADO_RK=n) into pado_inst_rkN.o

@@ -858,6 +858,7 @@ const char *pado_strerror(int s)
     case 2: return "n too small for this scheme (reference ierr 2)";
     case 3: return "n too small for periodic cd06 (reference ierr 3)";
     case 7: return "n too small for cf90 (reference ierr 7)";
+    case PADO_STAGG_E_SHORT: return "cd06stagg needs more than 4 points (reference exit code 21)";
     case PADO_E_BC: return "boundary specification must be 0, 1 or -1";
     case PADO_E_NULL: return "null handle or pointer";
     case PADO_E_ALIAS: return "input and output overlap";
