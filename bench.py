@@ -588,6 +588,7 @@ def run_single_op(args) -> None:
     op = {"cd06": pb.cd06, "cd10": pb.cd10, "cf90": pb.cf90}[scheme]()
     ierr = op.init(n, periodic) if scheme == "cf90" else op.init(n, 2 * np.pi / n, periodic, 0, 0)
     assert ierr == 0, ierr
+    op.set_variant(args.variant)
     g = torch.Generator(device="cuda").manual_seed(7)
     f = torch.randn(n1 * n2 * n3, dtype=torch.float64, device="cuda", generator=g)
     df = torch.empty_like(f)
@@ -642,6 +643,7 @@ def main() -> None:
     ap.add_argument("--bounded", action="store_true", help="profiling: bounded instead of periodic lines")
     ap.add_argument("--repeat", type=int, default=3, help="profiling: applications of the operator")
     ap.add_argument("--adjoint", action="store_true", help="profiling: the adjoint operator")
+    ap.add_argument("--variant", type=int, default=0, help="profiling: kernel variant (pado_set_kernel_variant)")
     ap.add_argument("--configs", action="store_true", help="the per-config table (C1-C3, GPU and CPU)")
     args = ap.parse_args()
     if args.configs:

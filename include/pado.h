@@ -174,8 +174,8 @@ int pado_apply_host_terms(const double *f_host, long n1, long n2, long n3, const
 int pado_set_tiling(pado_op_t op, int m, int lines);
 int pado_get_tiling(pado_op_t op, int *m, int *lines);
 /* Kernel organisation of the forward operator: 0 = automatic (the
- * streaming kernel where the field allows it; else 5 for x lines and cd06,
- * 1 otherwise, as measured fastest; the default),
+ * streaming kernel: 4 where the copy engine can move the field, else 6;
+ * adjoints of fields 4 cannot take run 1; the default),
  * 1 = one CTA per tile of lines, 2 = persistent CTAs that prefetch the next
  * tile with cp.async while the current one is solved, 3 = persistent CTAs
  * that read lines straight into registers and warm L2 with the next tile
@@ -185,9 +185,11 @@ int pado_get_tiling(pado_op_t op, int *m, int *lines);
  * PADO_E_UNSUPPORTED otherwise), 5 = the streaming kernel's resident tiles
  * fed by plain loads (any extent and alignment; a tile of 8 lines within
  * 110 KB of shared memory, i.e. n up to about 1300; PADO_E_UNSUPPORTED
- * otherwise).  Adjoints follow the same
- * choice (4 runs the transposed sweep in the tile, then B^T); 2, 3 and 5
- * mean 1 for adjoints.
+ * otherwise), 6 = the streaming kernel fed by per-element asynchronous
+ * copies (cp.async, 8 bytes each, landing on the stage's mbarrier): any
+ * extent, 8-byte aligned fields, forward operators.  Adjoints follow the
+ * same choice (4 runs the transposed sweep in the tile, then B^T); 2, 3, 5
+ * and 6 mean 1 for adjoints.
  * No counterpart in the reference (a B200 tuning knob). */
 int pado_set_kernel_variant(pado_op_t op, int variant);
 /* Tiling of the streaming kernel: lines per tile (8/16 for y/z lines,
@@ -203,7 +205,7 @@ int pado_set_stream_tiling(pado_op_t op, int lines, int stages);
  * memory); clear != 0 resets the word.  No counterpart in the reference. */
 int pado_device_status(pado_op_t op, int clear);
 /* The kernel a forward apply with these arguments would launch (nothing is
- * launched): info[0] kernel variant (1..4), [1] lines per tile, [2] stages,
+ * launched): info[0] kernel variant (1..6), [1] lines per tile, [2] stages,
  * [3] CTAs per SM, [4] segments per line, [5] coupling window, [6] threads
  * per CTA, [7] dynamic shared memory bytes.  No counterpart in the reference. */
 int pado_launch_plan(pado_op_t op, int kind, int axis, const double *f, double *df, long na, long nb, int bc1,

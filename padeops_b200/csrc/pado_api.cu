@@ -152,23 +152,30 @@ EncodeTiledFn encode_tiled()
     return fn;
 }
 
-StreamFn pick_stream(int rk, bool per, int m, bool xl, int lines, bool adj)
+StreamFn pick_stream(int rk, bool per, int m, bool xl, int lines, bool adj, bool as)
 {
     switch (rk) {
-    case RHS_CD06_D1: return pick_stream_rk0(per, m, xl, lines, adj);
-    case RHS_CD10_D1: return pick_stream_rk1(per, m, xl, lines, adj);
-    case RHS_CD10_D2: return pick_stream_rk2(per, m, xl, lines, adj);
-    default: return pick_stream_rk3(per, m, xl, lines, adj);
+    case RHS_CD06_D1: return pick_stream_rk0(per, m, xl, lines, adj, as);
+    case RHS_CD10_D1: return pick_stream_rk1(per, m, xl, lines, adj, as);
+    case RHS_CD10_D2: return pick_stream_rk2(per, m, xl, lines, adj, as);
+    default: return pick_stream_rk3(per, m, xl, lines, adj, as);
     }
 }
 
 int round16(long long v) { return (int)((v + 15) / 16 * 16); }
 
-// Doubles of one stage buffer: [L][n+2] (x lines) or nbox boxes of
-// box_rows x L (strided lines), rounded to 128 bytes.
-int stream_tile_doubles(bool xl, int n, int L)
+// Pitch of an x-line tile: n + 2 (rows 16-byte aligned) for the bulk copies;
+// the odd kp.P (n or n + 1) for per-element copies, so that the threads of a
+// warp, which sweep 16 different lines, hit different banks.
+int stream_xl_pitch(int n, bool as) { return as ? (n % 2 == 0 ? n + 1 : n) : n + 2; }
+
+// Doubles of one stage buffer: [L][pitch] (x lines), nbox boxes of
+// box_rows x L (strided lines, tensor copies) or n x L (strided lines,
+// per-element copies), rounded to 128 bytes.
+int stream_tile_doubles(bool xl, int n, int L, bool as)
 {
-    if (xl) return round16((long long)L * (n + 2));
+    if (xl) return round16((long long)L * stream_xl_pitch(n, as));
+    if (as) return round16((long long)n * L);
     const int nbox = (n + 255) / 256, box_rows = ((n + nbox - 1) / nbox + 15) / 16 * 16;
     return round16((long long)nbox * box_rows * L);
 }
@@ -203,9 +210,15 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     if (op->m != 16 && op->m != 32 && op->m != 64) return false;
     const bool xl = axis == 1;
     const size_t align_bits = reinterpret_cast<size_t>(kp0.in) | reinterpret_cast<size_t>(kp0.out);
-    if (align_bits & 15) return false;
-    if (xl ? (n % 2 != 0) : (na % 2 != 0 || na > 0x7fffffffLL || nb > 0x7fffffffLL)) return false;
+    if (na > 0x7fffffffLL || nb > 0x7fffffffLL) return false;
     if (kp0.nlines > 0x7fffffffLL) return false;  // tile indices are 32-bit in the kernel
+    // tensor / bulk copies need 16-byte aligned fields and an even extent along
+    // the contiguous axis (16-byte row strides); per-element asynchronous
+    // copies (variant 6, or the automatic choice when the copy engine cannot
+    // move the field) need 8-byte alignment and forward operators
+    const bool tma_ok = !(align_bits & 15) && (xl ? n % 2 == 0 : na % 2 == 0);
+    const bool as = op->variant == 6 || (op->variant == 0 && !tma_ok);
+    if (as ? (adj || (align_bits & 7)) : !tma_ok) return false;
     const int etab_rows = (int)(dt.host.etab.size() / E_NF), ktab_rows = (int)(dt.host.ktab.size() / KT_NF);
     // candidates in order of preference (measured on 512^3: 16 lines and one
     // stage, two CTAs per SM, is fastest for every operator); the first that
@@ -223,9 +236,9 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
         if (!xl && L == 32) continue;  // strided-line kernels exist for 8 and 16 lines per tile
         if (op->stream_lines && L != op->stream_lines) continue;
         if (op->stream_stages && stages != op->stream_stages) continue;
-        StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L, adj);
+        StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L, adj, as);
         if (!grant_smem(fn)) continue;
-        const int tile_doubles = stream_tile_doubles(xl, n, L);
+        const int tile_doubles = stream_tile_doubles(xl, n, L, as);
         const size_t bytes = stream_smem_bytes(L, S, kp0.xd, stages, tile_doubles, etab_rows, ktab_rows, resp_rows(kp0));
         if (bytes > 227 * 1024) continue;
         int ctas = 0;
@@ -247,14 +260,15 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     }
     if (!best_warps) return false;
     const int L = bestL, stages = best_stages;
-    const int tile_doubles = stream_tile_doubles(xl, n, L);
+    const int tile_doubles = stream_tile_doubles(xl, n, L, as);
     std::memset(sp, 0, sizeof(*sp));
     sp->kp = kp0;
     sp->kp.L = L;
     sp->kp.nslots = best_slots;
     std::memcpy(sp->kp.sperm, best_perm, sizeof(best_perm));
     sp->kp.border_slot = first_idle_slot(best_perm, best_slots);
-    sp->kp.P = xl ? n + 2 : kp0.P;  // x: rows 16-byte aligned for the bulk copies
+    sp->kp.P = xl ? stream_xl_pitch(n, as) : kp0.P;
+    sp->async_copy = as ? 1 : 0;
     sp->axis = axis;
     sp->stages = stages;
     sp->tile_doubles = tile_doubles;
@@ -267,6 +281,11 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     sp->status = op->d_status;
     if (xl) {
         sp->ntiles = (kp0.nlines + L - 1) / L;
+    } else if (as) {
+        sp->na = (int)na;
+        sp->xblocks = (int)((na + L - 1) / L);
+        sp->ntiles = (long long)sp->xblocks * nb;
+        sp->pstride = axis == 2 ? na * (long long)n : na;
     } else {
         // boxes of at most 256 rows; a multiple of 16 rows keeps every box's
         // shared-memory destination 128-byte aligned for any L
@@ -305,7 +324,7 @@ int sm_count()
 int launch_stream(pado_op_s *op, const StreamParams &sp, bool adj, int threads, size_t smem, int ctas_per_sm,
                   cudaStream_t st)
 {
-    StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1, sp.kp.L, adj);
+    StreamFn fn = pick_stream(sp.kp.rc.rk, op->periodic != 0, op->m, sp.axis == 1, sp.kp.L, adj, sp.async_copy != 0);
     const long long grid = std::min<long long>(sp.ntiles, (long long)ctas_per_sm * sm_count());
     if (grid < 1) return PADO_OK;
     fn<<<(unsigned)grid, threads, smem, st>>>(sp);
@@ -404,7 +423,7 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
         }
         return e == cudaSuccess ? PADO_OK : cuda_fail(e);
     }
-    if (op->variant == 0 || op->variant == 4) {
+    if (op->variant == 0 || op->variant == 4 || op->variant == 6) {
         const bool bounded_bc = !op->periodic && op->scheme != CD06;
         const int sb1 = solve_bc1 == SAME_BC ? bc1 : solve_bc1, sbn = solve_bcn == SAME_BC ? bcn : solve_bcn;
         const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? sb1 : 0, bounded_bc ? sbn : 0, adjoint ? 1 : 0));
@@ -413,7 +432,7 @@ int launch(pado_op_s *op, int kind, int axis, const double *f, double *df, long 
         size_t ssmem = 0;
         if (plan_stream(op, dt, kp, axis, na, nb, adjoint, &sp, &sthreads, &ssmem, &sctas))
             return launch_stream(op, sp, adjoint, sthreads, ssmem, sctas, st);
-        if (op->variant == 4) return PADO_E_UNSUPPORTED;
+        if (op->variant == 4 || (op->variant == 6 && !adjoint)) return PADO_E_UNSUPPORTED;
     }
     if ((op->variant == 5 || (op->variant == 0 && resident_fallback(op, axis))) && !adjoint && solve_bc1 == SAME_BC) {
         // the same resident tiles, with plain loads
@@ -778,7 +797,7 @@ int pado_set_tiling(pado_op_t op, int m, int lines)
 int pado_set_kernel_variant(pado_op_t op, int variant)
 {
     if (!op) return PADO_E_NULL;
-    if (variant < 0 || variant > 5) return PADO_E_ARG;
+    if (variant < 0 || variant > 6) return PADO_E_ARG;
     op->variant = variant;
     return PADO_OK;
 }
@@ -794,14 +813,14 @@ int pado_launch_plan(pado_op_t op, int kind, int axis, const double *f, double *
     if (rc != PADO_OK || trivial) return rc;
     info[4] = kp.S;
     info[5] = kp.W;
-    if (op->variant == 0 || op->variant == 4) {
+    if (op->variant == 0 || op->variant == 4 || op->variant == 6) {
         const bool bounded_bc = !op->periodic && op->scheme != CD06;
         const DevTables &dt = op->tables.at(TabKey(kind, bounded_bc ? bc1 : 0, bounded_bc ? bcn : 0, 0));
         StreamParams sp;
         int threads = 0, ctas = 0;
         size_t smem = 0;
         if (plan_stream(op, dt, kp, axis, na, nb, false, &sp, &threads, &smem, &ctas)) {
-            info[0] = 4;
+            info[0] = sp.async_copy ? 6 : 4;
             info[1] = sp.kp.L;
             info[2] = sp.stages;
             info[3] = ctas;

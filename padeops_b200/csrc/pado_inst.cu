@@ -40,29 +40,31 @@ KernelFn pick_m(int m, bool adj, bool contiguous, int variant)
     }
 }
 
-template <bool PER, bool XL, int LT, bool ADJ>
+template <bool PER, bool XL, int LT, bool ADJ, bool AS>
 StreamFn pick_stream_m(int m)
 {
     switch (m) {
-    case 16: return stream_kernel<RK, PER, 16, XL, LT, ADJ>;
-    case 32: return stream_kernel<RK, PER, 32, XL, LT, ADJ>;
-    default: return stream_kernel<RK, PER, 64, XL, LT, ADJ>;
+    case 16: return stream_kernel<RK, PER, 16, XL, LT, ADJ, AS>;
+    case 32: return stream_kernel<RK, PER, 32, XL, LT, ADJ, AS>;
+    default: return stream_kernel<RK, PER, 64, XL, LT, ADJ, AS>;
     }
 }
 
-template <bool PER, bool ADJ>
+template <bool PER, bool ADJ, bool AS>
 StreamFn pick_stream_l(int m, bool xl, int lines)
 {
-    if (xl) return pick_stream_m<PER, true, 0, ADJ>(m);
-    return lines == 8 ? pick_stream_m<PER, false, 8, ADJ>(m) : pick_stream_m<PER, false, 16, ADJ>(m);
+    if (xl) return pick_stream_m<PER, true, 0, ADJ, AS>(m);
+    return lines == 8 ? pick_stream_m<PER, false, 8, ADJ, AS>(m) : pick_stream_m<PER, false, 16, ADJ, AS>(m);
 }
 
 }  // namespace
 
-StreamFn PADO_CAT(pick_stream_rk, PADO_RK)(bool per, int m, bool xl, int lines, bool adj)
+// as: the tile copies are per-element cp.async (forward operators only)
+StreamFn PADO_CAT(pick_stream_rk, PADO_RK)(bool per, int m, bool xl, int lines, bool adj, bool as)
 {
-    if (adj) return per ? pick_stream_l<true, true>(m, xl, lines) : pick_stream_l<false, true>(m, xl, lines);
-    return per ? pick_stream_l<true, false>(m, xl, lines) : pick_stream_l<false, false>(m, xl, lines);
+    if (adj) return per ? pick_stream_l<true, true, false>(m, xl, lines) : pick_stream_l<false, true, false>(m, xl, lines);
+    if (as) return per ? pick_stream_l<true, false, true>(m, xl, lines) : pick_stream_l<false, false, true>(m, xl, lines);
+    return per ? pick_stream_l<true, false, false>(m, xl, lines) : pick_stream_l<false, false, false>(m, xl, lines);
 }
 
 KernelFn PADO_CAT(pick_kernel_rk, PADO_RK)(bool per, bool adj, bool contiguous, int m, int variant)

@@ -17,7 +17,16 @@
 // Strided lines (y, z): one 3-D tensor copy per box of {L lines, box_rows
 // rows} lands as the [row][L] tile.  Contiguous lines (x): one bulk copy per
 // line into a [L][P] tile (P = n + 2, rows 16-byte aligned), written back
-// by bulk stores.  The per-row table of the segments that read it and the
+// by bulk stores.
+//
+// Fields the copy engine cannot move (an odd extent along the contiguous
+// axis, or a pointer that is 8- but not 16-byte aligned) take the same
+// kernel with AS = true: every thread issues 8-byte asynchronous copies
+// (cp.async) of its share of the next tile and arrives on the stage's
+// mbarrier when they land (cp.async.mbarrier.arrive.noinc, one arrival per
+// thread), so the copies still run while the other CTAs on the SM compute.
+// x-line tiles then use an odd pitch P (no bank conflicts between lines)
+// and go back to global memory by coalesced stores from all threads.  The per-row table of the segments that read it and the
 // chain coefficients are staged in shared memory once per CTA.  Every wait
 // is bounded (2 s); on expiry the CTA records PADO_E_TIMEOUT in *status,
 // waits (bounded) for its copies in flight and returns.
@@ -36,8 +45,9 @@ namespace pado {
 constexpr int PADO_STATUS_TIMEOUT = -7;  // PADO_E_TIMEOUT of pado.h
 
 struct alignas(64) StreamParams {
-    CUtensorMap tmap;   // strided lines: 3-D view of the input field
+    CUtensorMap tmap;   // strided lines: 3-D view of the input field (TMA copies)
     KParams kp;
+    int async_copy;     // 1: the tile copies are per-element cp.async (AS kernels)
     long long ntiles;
     long long pstride;  // strided lines: elements between consecutive planes
     int na;             // strided lines: extent of the contiguous axis
@@ -203,6 +213,19 @@ __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.w
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
+// 8-byte asynchronous copy global -> shared (both addresses 8-byte aligned)
+__device__ __forceinline__ void async_copy8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+// arrive on the mbarrier once this thread's earlier cp.async copies have
+// landed (counts as one of the barrier's expected arrivals)
+__device__ __forceinline__ void async_arrive(unsigned long long *bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 constexpr unsigned long long STREAM_WAIT_NS = 2000000000ull;  // 2 s
 constexpr unsigned long long STREAM_DRAIN_NS = 200000000ull;  // 0.2 s
 
@@ -230,11 +253,66 @@ __device__ __forceinline__ void stream_issue_load(const StreamParams &sp, double
     }
 }
 
+// The copies of tile t into stage buffer `tile` by every thread of the CTA
+// (AS kernels): 8-byte cp.async of the thread's share, then one arrival on
+// the stage's mbarrier (initialised to the CTA's thread count).  Strided
+// lines: thread tid copies line tid % L, rows tid / L + k * (nthreads / L),
+// which lands at tile[tid + k * nthreads]; lines past the field are left
+// alone (their results are never stored).  x lines: the tile's lines are
+// consecutive in global memory, so element e of the tile's span goes to
+// row e % n of line e / n, at tile[(e / n) * P + e % n].
+template <bool XL, int LT>
+__device__ __forceinline__ void stream_issue_async(const StreamParams &sp, double *tile, unsigned long long *bar,
+                                                   long long t, int tid, int nthreads)
+{
+    const KParams &kp = sp.kp;
+    long long x0, p;
+    stream_tile_origin(sp, t, &x0, &p);
+    if (XL) {
+        const int n = kp.n, pad = kp.P - n;
+        const int total = stream_tile_lines(sp, t) * n;
+        const double *src = kp.in + x0 * (long long)n + tid;
+        const int l0 = tid / n;
+        int r = tid - l0 * n;
+        double *dst = tile + (size_t)l0 * kp.P + r;
+        const int dl = nthreads / n, dr = nthreads - dl * n;
+        const int dstep = dl * kp.P + dr;
+        for (int e = tid; e < total; e += nthreads) {
+            async_copy8(dst, src);
+            src += nthreads;
+            dst += dstep;
+            r += dr;
+            if (r >= n) {
+                r -= n;
+                dst += pad;
+            }
+        }
+    } else {
+        const int l = tid % LT;
+        if (x0 + l < sp.na) {
+            const int rstep = nthreads / LT;
+            const long long sstep = (long long)rstep * kp.stride;
+            const double *src = kp.in + (x0 + l) + p * sp.pstride + (long long)(tid / LT) * kp.stride;
+            double *dst = tile + tid;
+#pragma unroll 4
+            for (int r = tid / LT; r < kp.n; r += rstep) {
+                async_copy8(dst, src);
+                src += sstep;
+                dst += nthreads;
+            }
+        }
+    }
+    async_arrive(bar);
+}
+
 // LT: lines per tile for strided lines, fixed at compile time so that every
-// row offset in the [row][L] tile is an immediate (x lines: 0, L at run time)
-template <int RK, bool PER, int M, bool XL, int LT, bool ADJ = false>
+// row offset in the [row][L] tile is an immediate (x lines: 0, L at run time).
+// AS: the tile copies are per-element cp.async by all threads (any extent
+// and 8-byte alignment) instead of tensor / bulk copies.
+template <int RK, bool PER, int M, bool XL, int LT, bool ADJ = false, bool AS = false>
 __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ StreamParams sp)
 {
+    static_assert(!(AS && ADJ), "the adjoint streams by tensor / bulk copies only");
     using RL = ResidentLine<RK, PER, M, ADJ>;
     extern __shared__ double smem_raw[];
     // 1024-byte aligned base, by pointer arithmetic on the shared array so
@@ -267,7 +345,7 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     const long long ls = XL ? kp.P : 1;
 
     if (tid == 0) {
-        for (int b = 0; b < stages; ++b) mbar_init(&bars[b], 1);
+        for (int b = 0; b < stages; ++b) mbar_init(&bars[b], AS ? (unsigned)nthreads : 1u);
         mbar_fence_init();
     }
     stage_chain_table(kp, sm, tid, nthreads);
@@ -276,7 +354,13 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
     for (int i = tid; i < resp_rows(kp) * 2; i += nthreads) rtab[i] = __ldg(sp.rtab + i);
     for (int i = tid; i < S; i += nthreads) toff[i] = __ldg(sp.toff + i);
     __syncthreads();
-    if (tid == 0) {
+    if (AS) {
+        for (int b = 0; b < stages; ++b) {
+            const long long t = t_first + b * G;
+            if (t < sp.ntiles)
+                stream_issue_async<XL, LT>(sp, base + (size_t)b * sp.tile_doubles, &bars[b], t, tid, nthreads);
+        }
+    } else if (tid == 0) {
         for (int b = 0; b < stages; ++b) {
             const long long t = t_first + b * G;
             if (t < sp.ntiles) stream_issue_load(sp, base + (size_t)b * sp.tile_doubles, &bars[b], t);
@@ -302,7 +386,8 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
                         (void)mbar_wait(&bars[kk % stages], (unsigned)((kk / stages) & 1), STREAM_DRAIN_NS);
                 }
             }
-            if (XL) bulk_wait_all();
+            if (AS) async_wait_all();
+            else if (XL) bulk_wait_all();
             return;
         }
         sm.tile = base + (size_t)b * sp.tile_doubles;
@@ -339,7 +424,42 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
             if (active) RL::template fin<true>(kp, sm, line, rs, l, s, io.dst, io.ds, io.live, !XL);
         }
         const long long tn = t + (long long)stages * G;  // tile for this buffer next
-        if (XL && (!ADJ || adj_tile)) {
+        if (XL && AS) {
+            // the tile's lines are consecutive in global memory: coalesced
+            // stores of the whole span by all threads, in the output mode
+            __syncthreads();
+            const int n = kp.n, pad = kp.P - n;
+            const int total = stream_tile_lines(sp, t) * n;
+            double *dst = kp.out + x0 * (long long)n + tid;
+            const int l0 = tid / n;
+            int r = tid - l0 * n;
+            const double *src = sm.tile + (size_t)l0 * kp.P + r;
+            const int dl = nthreads / n, dr = nthreads - dl * n;
+            const int sstep = dl * kp.P + dr;
+            if (kp.out_mode == OUT_STORE) {
+                for (int e = tid; e < total; e += nthreads) {
+                    *dst = *src;
+                    dst += nthreads;
+                    src += sstep;
+                    r += dr;
+                    if (r >= n) {
+                        r -= n;
+                        src += pad;
+                    }
+                }
+            } else {
+                for (int e = tid; e < total; e += nthreads) {
+                    out_put(kp, dst, *src);
+                    dst += nthreads;
+                    src += sstep;
+                    r += dr;
+                    if (r >= n) {
+                        r -= n;
+                        src += pad;
+                    }
+                }
+            }
+        } else if (XL && (!ADJ || adj_tile)) {
             if (!ADJ && kp.out_mode != OUT_STORE) {
                 // scaled or accumulated output: the tile's lines take df's values
                 // (contiguous, read by whole warps) before they go out
@@ -370,9 +490,13 @@ __global__ void __launch_bounds__(384, 2) stream_kernel(const __grid_constant__ 
             }
         }
         __syncthreads();
-        if (tid == 0 && tn < sp.ntiles) stream_issue_load(sp, sm.tile, &bars[b], tn);
+        if (AS) {
+            if (tn < sp.ntiles) stream_issue_async<XL, LT>(sp, sm.tile, &bars[b], tn, tid, nthreads);
+        } else if (tid == 0 && tn < sp.ntiles) {
+            stream_issue_load(sp, sm.tile, &bars[b], tn);
+        }
     }
-    if (XL) bulk_wait_all();
+    if (XL && !AS) bulk_wait_all();
 }
 #endif  // __CUDACC__
 

@@ -101,7 +101,8 @@ class _Scheme:
     def set_variant(self, variant: int) -> None:
         """0 = automatic, 1 = one CTA per tile of lines, 2/3 = persistent CTAs
         with prefetch, 4 = the streaming (TMA-fed) kernel, 5 = its resident
-        tiles fed by plain loads (any extent and alignment)."""
+        tiles fed by plain loads, 6 = the streaming kernel fed by per-element
+        asynchronous copies (5 and 6: any extent and 8-byte alignment)."""
         check(L.lib().pado_set_kernel_variant(self.handle, variant), "set_variant")
 
     def launch_plan(self, kind: int, axis: int, f: torch.Tensor, df: torch.Tensor, na: int, nb: int,

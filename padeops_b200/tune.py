@@ -22,7 +22,7 @@ from . import _lib as L
 _CACHE_LOCK = threading.Lock()
 M_CHOICES = (16, 32, 64)
 LINE_CHOICES = (8, 16, 32)
-VARIANTS = (4, 5, 1, 2, 3)  # 4, 5: streaming kernel's resident tiles (they pick their own lines per tile)
+VARIANTS = (4, 6, 5, 1, 2, 3)  # 4, 6, 5: streaming kernel's resident tiles (they pick their own lines per tile)
 
 
 def cache_path() -> str:
@@ -90,7 +90,7 @@ def tune_op(op, kind: int, axis: int, shape: tuple[int, int, int], reps: int = 5
     for variant in VARIANTS:
         op.set_variant(variant)
         for m in M_CHOICES:
-            for lines in ((0,) if variant in (4, 5) else LINE_CHOICES):
+            for lines in ((0,) if variant in (4, 5, 6) else LINE_CHOICES):
                 try:
                     op.set_tiling(m, lines)
                     ms = time_op(op, kind, axis, f, df, na, nb, reps)

@@ -406,11 +406,11 @@ def test_field_operators(torch_cuda):
 
 @pytest.mark.parametrize("scheme,kind", OPS)
 def test_parity_resident_plain_loads(torch_cuda, scheme, kind):
-    """Variant 5 -- the resident tiles fed by plain loads, which the automatic
-    choice takes when the streaming kernel's copies cannot move the field (odd
-    extents, unaligned pointers) -- against the oracle, every axis, periodic and
-    bounded, odd and even extents, segments of 16, 32 and 64 rows, and an
-    unaligned field."""
+    """Variant 5 -- the resident tiles fed by plain loads -- and the automatic
+    choice, which streams fields the tensor copies cannot move (odd extents,
+    unaligned pointers) by per-element asynchronous copies (variant 6), against
+    the oracle: every axis, periodic and bounded, odd and even extents, segments
+    of 16, 32 and 64 rows, and an unaligned field."""
     torch = torch_cuda
     rng = np.random.default_rng(5 + scheme)
     for n, shape_of in ((33, lambda n: {1: (5, 7, n), 2: (5, n, 9), 3: (n, 7, 9)}),

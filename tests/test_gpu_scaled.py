@@ -25,14 +25,14 @@ def torch_cuda():
     return torch
 
 
-@pytest.mark.parametrize("variant", [0, 4, 5, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 4, 6, 5, 1, 2, 3])
 @pytest.mark.parametrize("periodic", [True, False])
 def test_scaled_and_accumulated(torch_cuda, variant, periodic):
     torch = torch_cuda
     rng = np.random.default_rng(7 + variant + 10 * periodic)
     for scheme, kind in OPS:
-        for n in (48, 256):
-            for axis, shape in ((1, (6, 5, n)), (2, (4, n, 22)), (3, (n, 5, 18))):
+        for n in (48, 49, 256):
+            for axis, shape in ((1, (6, 5, n)), (2, (4, n, 21 + n % 2)), (3, (n, 5, 17 + n % 2))):
                 f = rng.standard_normal(shape)
                 df0 = rng.standard_normal(shape)
                 op = _make(scheme, n, 0.2, periodic)
