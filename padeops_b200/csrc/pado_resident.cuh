@@ -32,7 +32,9 @@
 namespace pado {
 
 // fin with the launch's output mode (scaled / accumulated results), defined
-// after ResidentLine
+// after ResidentLine.  The shared-memory carve-up comes by value: by
+// reference, the caller keeps it in local memory for the call, and every
+// kernel then reads the tile through generic loads.
 template <int RK, bool PER, int M, bool ADJ, bool STAGED>
 #ifdef __CUDA_ARCH__
 __device__ __noinline__
@@ -40,7 +42,7 @@ __device__ __noinline__
 inline
 #endif
     void
-    fin_out_mode(const KParams &kp, const Smem &sm, const double *line, long long rs, int l, int s, double *out,
+    fin_out_mode(const KParams &kp, const Smem sm, const double *line, long long rs, int l, int s, double *out,
                  long long os);
 
 template <int RK, bool PER, int M, bool ADJ = false>
@@ -170,6 +172,139 @@ struct ResidentLine {
         }
     }
 
+    // ---- edge pieces of exactly E = M/2 rows (the layout cuts the rows
+    // outside the constant-coefficient block into such pieces): the per-row
+    // table path fully unrolled, every tile and table offset an immediate, no
+    // per-row bounds; the same arithmetic as the generic per-row loop.
+    static constexpr int E = M / 2;
+    static_assert(E >= 5, "the unrolled edge path needs pieces of at least 5 rows");
+
+    // the same address, marked for the compiler as shared memory (tile and
+    // staged tables), so that the unrolled paths load with shared-space
+    // instructions; the identity on the host
+    template <typename T>
+    static PADO_HD PADO_INLINE T *in_shared(T *q)
+    {
+#ifdef __CUDA_ARCH__
+        return reinterpret_cast<T *>(__cvta_shared_to_generic(__cvta_generic_to_shared(q)));
+#else
+        return q;
+#endif
+    }
+
+    // stencil + forward sweep of an edge piece (len == E); lenb < E only on
+    // the last segment of a cyclic line (its last nbord rows are the border)
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE void fwd_tab(const KParams &kp, const Smem &sm, double *p, long long rs, int l, int s,
+                                            int lenb, double (&w)[9], const Halo &h)
+    {
+        const bool first = !PER && s == 0, last = !PER && s == kp.S - 1;  // last: the piece ends at row n
+        p = in_shared(p);
+        if (!ADJ) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) w[4 + k] = p[(long long)k * rs];
+        }
+        const double *tb = in_shared(seg_etab(sm, s));
+        double cst[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) cst[k] = kp.rc.c[k];
+        double z1 = 0.0, z2 = 0.0, s1 = 0.0, s2 = 0.0, rb0 = 0.0, rb1 = 0.0;
+#pragma unroll
+        for (int t = 0; t < E; ++t) {
+            double r;
+            if (ADJ) {
+                r = p[(long long)t * rs];
+            } else {
+                r = rhs_interior_fma(RK, PER, cst, w);
+                if (t < CR && first) r = h.cv[t < CR ? t : 0];
+                if (t >= E - CR && last) r = h.cl[t >= E - CR ? t - (E - CR) : 0];
+            }
+            if (!CYC || t < E - 2 || t < lenb) {
+                const double *tr = tb + (size_t)t * E_NF;
+                const Dbl2 cc = tld2<STAGED>(tr + E_C1);
+                const Dbl2 ak = (HAS_ALPHA || CYC) ? tld2<STAGED>(tr + E_ALPHA) : Dbl2{1.0, 0.0};
+                double z = HAS_ALPHA ? ak.x * r : r;
+                if (ORDER2) z -= cc.y * z2;
+                z -= cc.x * z1;
+                p[(long long)t * rs] = z;
+                if (CYC) {
+                    s1 += ak.y * z;
+                    if (ORDER2) s2 += tld<STAGED>(tr + E_K2) * z;
+                }
+                z2 = z1;
+                z1 = z;
+            } else {
+                // border rows of a cyclic line: right-hand sides only
+                if (t == lenb) rb0 = r;
+                else rb1 = r;
+            }
+            if (!ADJ) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) w[k] = w[k + 1];
+                if (t + 5 < E) w[8] = p[(long long)(t + 5 < E ? t + 5 : 0) * rs];
+                else if (t + 5 - E < 4) w[8] = h.hn[t + 5 - E < 4 ? t + 5 - E : 0];
+            }
+        }
+        LK::template summarize_fwd<STAGED>(kp, sm, l, s, z1, z2, s1, s2);
+        if (CYC && s == kp.S - 1) {
+            sm.eb[(size_t)l * 4 + 2] = rb0;
+            sm.eb[(size_t)l * 4 + 3] = rb1;
+        }
+    }
+
+    // backward sweep of an edge piece, x written over z; returns the piece's
+    // first two x
+    template <bool STAGED>
+    static PADO_HD PADO_INLINE Dbl2 bwd_tab(const Smem &sm, double *p, long long rs, int s, int lenb, double P1,
+                                            double P2)
+    {
+        double x1 = 0.0, x2 = 0.0;
+        p = in_shared(p);
+        const double *tb = in_shared(seg_etab(sm, s));
+#pragma unroll
+        for (int t = E - 1; t >= 0; --t) {
+            if (CYC && t >= E - 2 && t >= lenb) continue;  // border rows
+            const double *tr = tb + (size_t)t * E_NF;
+            const Dbl2 uv = tld2<STAGED>(tr + E_U);
+            const Dbl2 gd = tld2<STAGED>(tr + E_GAMMA);
+            double z = p[(long long)t * rs] + P1 * uv.x;
+            if (ORDER2) z += P2 * uv.y;
+            double x = gd.x * z;
+            if (ORDER2) x -= tld<STAGED>(tr + E_D2) * x2;
+            x -= gd.y * x1;
+            p[(long long)t * rs] = x;
+            x2 = x1;
+            x1 = x;
+        }
+        return Dbl2{x1, x2};
+    }
+
+    // corrected x of an edge piece -> out
+    template <bool STAGED, bool XF>
+    static PADO_HD PADO_INLINE void fin_tab(const KParams &kp, const Smem &sm, const double *p, long long rs, double *q,
+                                            long long os, int a, int s, int lenb, double Q1, double Q2, double E1,
+                                            double E2, bool spike_rows)
+    {
+        p = in_shared(p);
+        const double *tb = in_shared(seg_etab(sm, s));
+        const double *rtab = in_shared(sm.rtab);
+#pragma unroll
+        for (int t = 0; t < E; ++t) {
+            if (CYC && t >= E - 2 && t >= lenb) continue;  // border rows
+            const Dbl2 stt = tld2<STAGED>(tb + (size_t)t * E_NF + E_S);
+            double x = p[(long long)t * rs] + Q1 * stt.x;
+            if (ORDER2) x += Q2 * stt.y;
+            if (spike_rows && (a + t < kp.ie || a + t >= kp.je)) {
+                const double *rr = resp_row(kp, rtab, a + t);
+                x += E1 * rr[0];
+                if (ORDER2) x += E2 * rr[1];
+            }
+            if (HAS_DELTA) x *= tld<STAGED>(tb + (size_t)t * E_NF + E_DELTA);
+            if (XF) out_put(kp, q + (long long)t * os, x);
+            else q[(long long)t * os] = x;
+        }
+    }
+
     // ---- fwd: stencil + local forward sweep, z written over f ---------------
     template <bool STAGED>
     static PADO_HD PADO_INLINE void fwd(const KParams &kp, const Smem &sm, double *line, long long rs, int l, int s,
@@ -191,6 +326,10 @@ struct ResidentLine {
             // that the common path carries no per-row predicates
             if (CYC && ((kp.spk_mask >> s) & 1u)) fwd_fast<STAGED, true>(kp, sm, p, rs, l, s, a, w, h);
             else fwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, w, h);
+            return;
+        }
+        if (len == E) {
+            fwd_tab<STAGED>(kp, sm, p, rs, l, s, lenb, w, h);
             return;
         }
         if (!ADJ) {
@@ -354,6 +493,10 @@ struct ResidentLine {
         if (CYC && s == 0 && kp.border_slot < 0) border_only(kp, sm, l);
         if (fast(kp, s)) {
             bwd_fast<STAGED, false>(kp, sm, p, rs, l, s, a, P1, P2, 0.0, 0.0, x1, x2);
+        } else if (len == E) {
+            const Dbl2 xx = bwd_tab<STAGED>(sm, p, rs, s, lenb, P1, P2);
+            x1 = xx.x;
+            x2 = xx.y;
         } else {
             const double *tb = seg_etab(sm, s);
 #pragma unroll 1
@@ -444,6 +587,9 @@ struct ResidentLine {
             return;
         }
         const double *tb = seg_etab(sm, s);
+        if (len == E) {
+            fin_tab<STAGED, XF>(kp, sm, p, rs, q, os, a, s, lenb, Q1, Q2, E1, E2, spike_rows);
+        } else {
 #pragma unroll 2
         for (int t = 0; t < lenb; ++t) {
             const Dbl2 stt = tld2<STAGED>(tb + (size_t)t * E_NF + E_S);
@@ -457,6 +603,7 @@ struct ResidentLine {
             if (HAS_DELTA) x *= tld<STAGED>(tb + (size_t)t * E_NF + E_DELTA);
             if (XF) out_put(kp, q + (long long)t * os, x);
             else q[(long long)t * os] = x;
+        }
         }
         if (CYC && s == kp.S - 1) {
             if (XF) {
@@ -580,7 +727,7 @@ __device__ __noinline__
 inline
 #endif
     void
-    fin_out_mode(const KParams &kp, const Smem &sm, const double *line, long long rs, int l, int s, double *out,
+    fin_out_mode(const KParams &kp, const Smem sm, const double *line, long long rs, int l, int s, double *out,
                  long long os)
 {
     ResidentLine<RK, PER, M, ADJ>::template fin_body<STAGED, true>(kp, sm, line, rs, l, s, out, os);

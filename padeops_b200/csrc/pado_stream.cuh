@@ -288,14 +288,15 @@ __device__ __forceinline__ void stream_issue_async(const StreamParams &sp, doubl
             }
         }
     } else {
-        const int l = tid % LT;
+        constexpr int LS = LT > 0 ? LT : 1;  // LT is 0 only in x-line kernels, which never get here
+        const int l = tid % LS;
         if (x0 + l < sp.na) {
-            const int rstep = nthreads / LT;
+            const int rstep = nthreads / LS;
             const long long sstep = (long long)rstep * kp.stride;
-            const double *src = kp.in + (x0 + l) + p * sp.pstride + (long long)(tid / LT) * kp.stride;
+            const double *src = kp.in + (x0 + l) + p * sp.pstride + (long long)(tid / LS) * kp.stride;
             double *dst = tile + tid;
 #pragma unroll 4
-            for (int r = tid / LT; r < kp.n; r += rstep) {
+            for (int r = tid / LS; r < kp.n; r += rstep) {
                 async_copy8(dst, src);
                 src += sstep;
                 dst += nthreads;

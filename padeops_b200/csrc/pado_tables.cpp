@@ -394,18 +394,42 @@ Layout make_layout(int n, int m, int i0, int i1)
         L.st.assign(L.S + 1, 0);
         for (int s = 0; s <= L.S; ++s) L.st[s] = (int)((long long)n * s / L.S);
     };
-    const int A = std::max(i0, HALO), B = std::min(i1, n - HALO);
-    int k = (i0 < i1 && B > A) ? (B - A) / m : 0;
-    if (k < 1 || m < 8) {
+    const int A0 = std::max(i0, HALO), B = std::min(i1, n - HALO);
+    const int kmax = (i0 < i1 && B > A0) ? (B - A0) / m : 0;
+    if (kmax < 1 || m < 8) {
         uniform((n + m - 1) / m);
         return L;
     }
-    // pieces of at most e rows, at least 4, on each side of the interior block
+    // Lines whose length is a multiple of E = m/2: pieces of exactly E rows
+    // before and after the interior block, which the kernels run on a fully
+    // unrolled per-row-table path (about as fast per row as the interior);
+    // the block of k interior segments starts at a whole number of pieces
+    // (one interior segment fewer where the rounding needs it).
+    const int E = m / 2;
+    if (n % E == 0) {
+        const int A = (A0 + E - 1) / E * E;
+        for (int k = kmax; k >= std::max(1, kmax - 1); --k) {
+            if (A + k * m > B) continue;
+            std::vector<int> st;
+            for (int r = 0; r < A; r += E) st.push_back(r);
+            for (int j = 0; j < k; ++j) st.push_back(A + j * m);
+            for (int r = A + k * m; r < n; r += E) st.push_back(r);
+            st.push_back(n);
+            if ((int)st.size() - 1 > MAX_SEGMENTS) break;
+            L.st = st;
+            L.S = (int)st.size() - 1;
+            return L;
+        }
+    }
+    // otherwise pieces of about m/3 rows (near-equal), on the generic per-row
+    // loop, several times slower per row than the interior: short pieces keep
+    // every thread of a tile near an interior segment's time
+    int k = kmax;
     int e = std::max(4, (m + 2) / 3);
     auto pieces = [](int rows, int e_) { return rows <= 0 ? 0 : (rows + e_ - 1) / e_; };
     for (;;) {
-        const int right = n - (A + k * m);
-        const int S = k + pieces(A, e) + pieces(right, e);
+        const int right = n - (A0 + k * m);
+        const int S = k + pieces(A0, e) + pieces(right, e);
         if (S <= MAX_SEGMENTS) break;
         if (e < m) ++e;
         else if (k > 1) --k;
@@ -419,9 +443,9 @@ Layout make_layout(int n, int m, int i0, int i1)
         const int np = pieces(hi - lo, e);
         for (int j = 0; j < np; ++j) L.st.push_back(lo + (int)((long long)(hi - lo) * j / np));
     };
-    cut(0, A);
-    for (int j = 0; j < k; ++j) L.st.push_back(A + j * m);
-    cut(A + k * m, n);
+    cut(0, A0);
+    for (int j = 0; j < k; ++j) L.st.push_back(A0 + j * m);
+    cut(A0 + k * m, n);
     L.st.push_back(n);
     L.S = (int)L.st.size() - 1;
     return L;
@@ -750,12 +774,15 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
 int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots, bool border_warp)
 {
     const int S = ot.lay.S;
+    // code-path classes: per-row table unrolled (pieces of m/2 rows), per-row
+    // table loop (other lengths), then the interior with or without spike sums
+    // and border responses
     auto cls = [&](int s) {
-        if (!((ot.interior.mask >> s) & 1u)) return 0;
-        const bool spk = (ot.interior.spk_mask >> s) & 1u;
         const int a = ot.lay.start(s), len = ot.lay.len(s);
+        if (!((ot.interior.mask >> s) & 1u)) return len == ot.m / 2 ? 0 : 1;
+        const bool spk = (ot.interior.spk_mask >> s) & 1u;
         const bool resp = ot.nbord > 0 && (a < ot.ie || a + len > ot.je);
-        return spk ? (resp ? 1 : 2) : (resp ? 3 : 4);
+        return spk ? (resp ? 2 : 3) : (resp ? 4 : 5);
     };
     const int spw = L >= 32 ? 1 : 32 / L;
     int k = 0;
@@ -763,7 +790,7 @@ int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots, b
         // a warp of idle slots first: its first slot is the first idle one
         for (int j = 0; j < spw && k < max_slots; ++j) sperm[k++] = 0xff;
     }
-    for (int c = 0; c <= 4; ++c) {
+    for (int c = 0; c <= 5; ++c) {
         int cnt = 0;
         for (int s = 0; s < S; ++s)
             if (cls(s) == c) {

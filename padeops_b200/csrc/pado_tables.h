@@ -42,10 +42,10 @@ struct Layout {
     int len(int s) const { return st[s + 1] - st[s]; }
 };
 // With an interior [i0, i1) (i0 < i1): as many segments of exactly m rows as
-// fit in it, and the rows before and after cut into short pieces (about m/3
-// rows: they run the per-row-table path, about three times slower per row),
-// so that every thread of a tile finishes at about the same time.  Without
-// one: ceil(n/m) segments of near-equal length.
+// fit in it, and the rows before and after cut into pieces of m/2 rows (the
+// kernels' fully unrolled per-row-table path) when n is a multiple of m/2,
+// else into near-equal pieces of about m/3 rows (the generic per-row loop).
+// Without one: ceil(n/m) segments of near-equal length.
 constexpr int MAX_SEGMENTS = 32;
 Layout make_layout(int n, int m, int i0 = 0, int i1 = 0);
 // Banded rows [i0, i1) whose coefficients have settled (see Interior);
