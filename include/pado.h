@@ -250,6 +250,11 @@ int pado_batch_set_graph_branches(pado_batch_t batch, int branches);
 int pado_batch_set_config(pado_batch_t batch, int lines, int ctas_per_sm);
 /* Tiles, grid size, threads per CTA and dynamic shared memory of the batch. */
 int pado_batch_info(pado_batch_t batch, long long *ntiles, int *grid, int *threads, long long *smem_bytes);
+/* Device-side status of the batch's last persistent launch: PADO_OK, or
+ * PADO_E_TIMEOUT when a CTA's bounded wait for its tile copies expired (that
+ * CTA stopped; the outputs are incomplete).  Synchronous.  No counterpart in
+ * the reference. */
+int pado_batch_status(pado_batch_t batch);
 void pado_batch_destroy(pado_batch_t batch);
 
 /* Most items one pado_batch_run_static call accepts. */

@@ -73,6 +73,7 @@ SIGNATURES = {
     "pado_batch_set_config": (_I, [_P, _I, _I]),
     "pado_batch_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I), ctypes.POINTER(_I),
                              ctypes.POINTER(ctypes.c_longlong)]),
+    "pado_batch_status": (_I, [_P]),
     "pado_batch_destroy": (None, [_P]),
     "pado_batch_run_static": (_I, [_P, _I, _P]),
     "pado_batch_set_graph_branches": (_I, [_P, _I]),

@@ -59,6 +59,11 @@ class Batch:
         """Lines per tile (8, 16, 32, 64; 0 = automatic) and a cap on CTAs per SM (0 = none)."""
         return L.lib().pado_batch_set_config(self._h, lines, ctas_per_sm)
 
+    def status(self) -> int:
+        """Device status of the last persistent launch: 0, or E_TIMEOUT when a
+        CTA's bounded wait for its tile copies expired (synchronous)."""
+        return L.lib().pado_batch_status(self._h)
+
     def info(self) -> dict:
         nt, grid, thr, smem = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
         check(L.lib().pado_batch_info(self._h, ctypes.byref(nt), ctypes.byref(grid), ctypes.byref(thr),

@@ -216,7 +216,7 @@ int upload_batch(pado_batch_s *b)
         if (e != cudaSuccess) return cuda_fail(e);
     }
     if (!b->d_counter) {
-        cudaError_t e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
+        cudaError_t e = cudaMalloc(&b->d_counter, 2 * sizeof(unsigned long long));
         if (e != cudaSuccess) return cuda_fail(e);
     }
     // The attribute is per function, shared by every batch: always the cap (every
@@ -246,7 +246,7 @@ void drop_graph(pado_batch_s *b)
 int enqueue_persistent(pado_batch_s *b, cudaStream_t st)
 {
     if (b->ntiles == 0) return PADO_OK;
-    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), st);
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return cuda_fail(e);
     batch_kernel<<<b->grid, BATCH_THREADS, b->smem, st>>>(b->d_items, b->d_tile0s, (int)b->dev.size(), b->ntiles,
                                                           b->d_counter);
@@ -419,7 +419,7 @@ void pado_batch_destroy(pado_batch_t b)
 
 // ---- the batched launch without device allocation --------------------------
 //
-// g_static_batch holds the tile counter (first 256 bytes), the item
+// g_static_batch holds the tile counter and the status word (first 256 bytes), the item
 // descriptors and their first tiles.  Host code must not use its name as an
 // address: the device address comes from cudaGetSymbolAddress, once per
 // device.
@@ -535,7 +535,7 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
     const long long ntiles = t0;
     e = cudaMemcpyAsync(d_tile0s, starts, (size_t)nvalid * sizeof(long long), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(e);
-    e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st);
+    e = cudaMemsetAsync(d_counter, 0, 2 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return cuda_fail(e);
 
     e = cudaFuncSetAttribute((const void *)batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -552,6 +552,16 @@ int pado_batch_run_static(const pado_batch_item *items, int nitems, void *stream
     g_launches.fetch_add(1, std::memory_order_relaxed);
     e = cudaGetLastError();
     return e == cudaSuccess ? PADO_OK : cuda_fail(e);
+}
+
+int pado_batch_status(pado_batch_t b)
+{
+    if (!b) return PADO_E_NULL;
+    if (!b->d_counter) return PADO_OK;
+    unsigned long long v[2] = {0, 0};
+    cudaError_t e = cudaMemcpy(v, b->d_counter, sizeof(v), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e);
+    return (int)(long long)v[1];
 }
 
 int pado_batch_info(pado_batch_t b, long long *ntiles, int *grid, int *threads, long long *smem_bytes)

@@ -68,6 +68,28 @@ def test_batch_parity(mode):
             it[4].fill_(float("nan"))
         getattr(b, mode)()
         _check(torch, items, host)
+        if mode != "run_loop":
+            assert b.status() == 0
+    b.destroy()
+
+
+@pytest.mark.parametrize("mode", ["run", "run_graph"])
+def test_batch_odd_extents(mode):
+    """Odd extents along every axis (the persistent launch copies tiles element
+    by element, so no extent or alignment rule applies), partial tiles, many
+    tiles per CTA."""
+    import torch
+
+    from padeops_b200.batch import Batch
+
+    items, host = _items(torch, 40, seed=31, dims=(31, 48, 65, 97, 127))
+    b = Batch(items)
+    for _ in range(2):
+        for it in items:
+            it[4].fill_(float("nan"))
+        getattr(b, mode)()
+        _check(torch, items, host)
+        assert b.status() == 0
     b.destroy()
 
 
