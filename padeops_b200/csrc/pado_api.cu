@@ -86,6 +86,10 @@ int build_tables(pado_op_s *op)
     for (void *p : op->allocations) cudaFree(p);
     op->allocations.clear();
     op->tables.clear();
+    {
+        std::lock_guard<std::mutex> g(op->plan_mu);
+        op->plan_cache.clear();  // its keys name the tables
+    }
     const int n = op->n;
     if (n == 1) return PADO_OK;
     std::vector<int> kinds;
@@ -203,39 +207,25 @@ bool grant_smem(StreamFn fn)
 // when the field or tiling does not fit it (odd strides, unaligned pointers,
 // a table too large to stage); the caller then runs the one-CTA-per-tile
 // kernel.
-bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, int axis, long long na, long long nb,
-                 bool adj, StreamParams *sp, int *threads, size_t *smem, int *ctas_per_sm)
+// The streaming kernel's tiling for one (tables, direction, copy path).  The
+// candidates are tried in order of preference (16 lines and one stage, two
+// CTAs per SM, is fastest for every operator at n = 512; a larger tile only
+// pays for short x lines); the first that fits two CTAs per SM wins, else the
+// one with the most resident warps.  One exception, measured on x lines of
+// 64 to 256 points: 32 lines per tile beat 16 by 4-22% whenever they keep at
+// least as many threads resident (two CTAs or more per SM).
+bool choose_stream_tiling(const pado_op_s *op, const DevTables &dt, const KParams &kp0, bool xl, bool as, bool adj,
+                          int etab_rows, int ktab_rows, StreamChoice *out)
 {
     const int n = op->n, S = kp0.S;
-    if (op->m != 16 && op->m != 32 && op->m != 64) return false;
-    const bool xl = axis == 1;
-    const size_t align_bits = reinterpret_cast<size_t>(kp0.in) | reinterpret_cast<size_t>(kp0.out);
-    if (na > 0x7fffffffLL || nb > 0x7fffffffLL) return false;
-    if (kp0.nlines > 0x7fffffffLL) return false;  // tile indices are 32-bit in the kernel
-    // tensor / bulk copies need 16-byte aligned fields and an even extent along
-    // the contiguous axis (16-byte row strides); per-element asynchronous
-    // copies (variant 6, or the automatic choice when the copy engine cannot
-    // move the field) need 8-byte alignment and forward operators
-    const bool tma_ok = !(align_bits & 15) && (xl ? n % 2 == 0 : na % 2 == 0);
-    // x lines of bounded operators and of cd06 run faster from the odd-pitch
-    // tile the per-element copies fill (no bank conflicts between the lines a
-    // warp sweeps) than from the bulk copies' even pitch: measured on 512^3,
-    // 2.5-17% (bounded), 7% (periodic cd06); periodic cd10 / cf90 x lines
-    // lose 4-7% with them and keep the bulk copies
-    const bool prefer_async = xl && !adj && (!op->periodic || op->scheme == CD06);
-    const bool as_ok = !adj && !(align_bits & 7);
-    bool as = op->variant == 6 || (op->variant == 0 && (!tma_ok || prefer_async));
-    if (as && !as_ok && op->variant == 0 && tma_ok) as = false;
-    if (as ? !as_ok : !tma_ok) return false;
-    const int etab_rows = (int)(dt.host.etab.size() / E_NF), ktab_rows = (int)(dt.host.ktab.size() / KT_NF);
-    // candidates in order of preference (measured on 512^3: 16 lines and one
-    // stage, two CTAs per SM, is fastest for every operator); the first that
-    // fits two CTAs per SM wins, else the one with the most resident warps
-    int best_warps = 0, bestL = 0, best_stages = 0, best_ctas = 0, best_slots = 0;
-    unsigned char best_perm[KMAXSLOT] = {0};
+    struct Cand {
+        StreamChoice c;
+        bool ok = false;
+    };
     const int cand[6][2] = {{16, 1}, {32, 1}, {8, 1}, {16, 2}, {32, 2}, {8, 2}};
-    for (const auto &c : cand) {
-        const int L = c[0], stages = c[1];
+    Cand res[6];
+    for (int i = 0; i < 6; ++i) {
+        const int L = cand[i][0], stages = cand[i][1];
         // slots grouped by code path, padded to whole warps
         unsigned char perm[KMAXSLOT];
         int nslots = warp_slots(dt.host, L, perm, KMAXSLOT, true);
@@ -255,19 +245,80 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
             continue;
         }
         if (ctas < 1) continue;
-        const int warps = ctas * ((L * nslots + 31) / 32);
-        if (ctas >= 2 || warps > best_warps) {
-            best_warps = warps;
-            bestL = L;
-            best_stages = stages;
-            best_ctas = ctas;
-            best_slots = nslots;
-            std::memcpy(best_perm, perm, sizeof(perm));
-            if (ctas >= 2) break;
+        res[i].ok = true;
+        res[i].c.L = L;
+        res[i].c.stages = stages;
+        res[i].c.ctas = ctas;
+        res[i].c.nslots = nslots;
+        std::memcpy(res[i].c.perm, perm, sizeof(perm));
+    }
+    auto resident = [&](int i) { return (long long)res[i].c.ctas * res[i].c.L * res[i].c.nslots; };
+    int pick = -1;
+    for (int i = 0; i < 6 && pick < 0; ++i)
+        if (res[i].ok && res[i].c.ctas >= 2) pick = i;
+    if (pick == 0 && xl && res[1].ok && res[1].c.ctas >= 2 && resident(1) >= resident(0)) pick = 1;
+    if (pick < 0) {
+        long long best = -1;
+        for (int i = 0; i < 6; ++i)
+            if (res[i].ok && resident(i) > best) {
+                best = resident(i);
+                pick = i;
+            }
+    }
+    if (pick < 0) return false;
+    *out = res[pick].c;
+    return true;
+}
+
+bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, int axis, long long na, long long nb,
+                 bool adj, StreamParams *sp, int *threads, size_t *smem, int *ctas_per_sm)
+{
+    const int n = op->n, S = kp0.S;
+    if (op->m != 16 && op->m != 32 && op->m != 64) return false;
+    const bool xl = axis == 1;
+    const size_t align_bits = reinterpret_cast<size_t>(kp0.in) | reinterpret_cast<size_t>(kp0.out);
+    if (na > 0x7fffffffLL || nb > 0x7fffffffLL) return false;
+    if (kp0.nlines > 0x7fffffffLL) return false;  // tile indices are 32-bit in the kernel
+    // tensor / bulk copies need 16-byte aligned fields and an even extent along
+    // the contiguous axis (16-byte row strides); per-element asynchronous
+    // copies (variant 6, or the automatic choice when the copy engine cannot
+    // move the field) need 8-byte alignment and forward operators
+    const bool tma_ok = !(align_bits & 15) && (xl ? n % 2 == 0 : na % 2 == 0);
+    // Some x lines run faster from the odd-pitch tile the per-element copies
+    // fill (no bank conflicts between the lines a warp sweeps) than from the
+    // bulk copies' even pitch.  Measured (B200, lines of 128 to 1024 points):
+    // cd06 for n = 128..512 (4-17% faster), bounded cd10 d1 and cf90 for
+    // n = 256..512 (2-9%); every other case, and every n = 1024, is 3-19%
+    // slower with them and keeps the bulk copies.
+    const bool bounded10 = !op->periodic && op->scheme != CD06 && kp0.rc.rk != RHS_CD10_D2;
+    const bool prefer_async =
+        xl && !adj && ((op->scheme == CD06 && n >= 128 && n <= 512) || (bounded10 && n >= 256 && n <= 512));
+    const bool as_ok = !adj && !(align_bits & 7);
+    bool as = op->variant == 6 || (op->variant == 0 && (!tma_ok || prefer_async));
+    if (as && !as_ok && op->variant == 0 && tma_ok) as = false;
+    if (as ? !as_ok : !tma_ok) return false;
+    const int etab_rows = (int)(dt.host.etab.size() / E_NF), ktab_rows = (int)(dt.host.ktab.size() / KT_NF);
+    const PlanKey pkey(&dt, xl ? 1 : 0, as ? 1 : 0, adj ? 1 : 0, op->stream_lines, op->stream_stages);
+    StreamChoice choice;
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> g(op->plan_mu);
+        auto it = op->plan_cache.find(pkey);
+        if (it != op->plan_cache.end()) {
+            choice = it->second;
+            cached = true;
         }
     }
-    if (!best_warps) return false;
-    const int L = bestL, stages = best_stages;
+    if (!cached) {
+        if (!choose_stream_tiling(op, dt, kp0, xl, as, adj, etab_rows, ktab_rows, &choice)) return false;
+        std::lock_guard<std::mutex> g(op->plan_mu);
+        op->plan_cache[pkey] = choice;
+    }
+    const int best_slots = choice.nslots, best_ctas = choice.ctas;
+    unsigned char best_perm[KMAXSLOT];
+    std::memcpy(best_perm, choice.perm, sizeof(best_perm));
+    if (!grant_smem(pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, choice.L, adj, as))) return false;
+    const int L = choice.L, stages = choice.stages;
     const int tile_doubles = stream_tile_doubles(xl, n, L, as);
     std::memset(sp, 0, sizeof(*sp));
     sp->kp = kp0;

@@ -37,6 +37,16 @@ struct DevTables {
 
 using TabKey = std::tuple<int, int, int, int>;  // kind, bc1, bcn, adjoint
 
+// The streaming kernel's tiling for one (tables, line direction, copy path,
+// direction of the solve, requested tiling) of a handle, chosen once by the
+// planner: lines per tile, stages, CTAs per SM, thread slots and their
+// segments.
+struct StreamChoice {
+    int L = 0, stages = 0, ctas = 0, nslots = 0;
+    unsigned char perm[KMAXSLOT] = {0};
+};
+using PlanKey = std::tuple<const void *, int, int, int, int, int>;  // tables, x lines, async, adjoint, lines, stages
+
 int cuda_fail(cudaError_t e);
 bool kind_supported(int scheme, int kind);
 bool valid_bc(int bc);
@@ -51,6 +61,8 @@ struct pado_op_s {
     int device = 0;
     int *d_status = nullptr;  // device-side status word (bounded waits)
     int stream_lines = 0, stream_stages = 0;  // streaming kernel tiling (0: chosen by occupancy)
+    mutable std::mutex plan_mu;                                      // guards plan_cache
+    mutable std::map<pado::PlanKey, pado::StreamChoice> plan_cache;  // the planner's choices
     std::map<pado::TabKey, pado::DevTables> tables;
     std::vector<void *> allocations;
     // host-buffer staging

@@ -131,7 +131,6 @@ PADO_HD PADO_INLINE LineIO stream_line_io_at(const StreamParams &sp, const Smem 
 
 PADO_HD PADO_INLINE LineIO stream_line_io(const StreamParams &sp, const Smem &sm, int l, long long t)
 {
-    const KParams &kp = sp.kp;
     long long x0, p;
     stream_tile_origin(sp, t, &x0, &p);
     return stream_line_io_at(sp, sm, l, x0, p);
