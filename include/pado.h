@@ -192,9 +192,9 @@ int pado_get_tiling(pado_op_t op, int *m, int *lines);
  * and 6 mean 1 for adjoints.
  * No counterpart in the reference (a B200 tuning knob). */
 int pado_set_kernel_variant(pado_op_t op, int variant);
-/* Tiling of the streaming kernel: lines per tile (8/16 for y/z lines,
- * 8/16/32 for x lines) and shared-memory stages (1 or 2); 0 leaves the
- * choice to the occupancy-based planner (the default).  A fixed choice that
+/* Tiling of the streaming kernel: lines per tile (8, 16 or 32) and
+ * shared-memory stages (1 or 2); 0 leaves the choice to the
+ * occupancy-based planner (the default).  A fixed choice that
  * does not fit makes the forward operator fall back to variant 1 (variant 0)
  * or fail with PADO_E_UNSUPPORTED (variant 4).  No counterpart in the
  * reference (a B200 tuning knob). */

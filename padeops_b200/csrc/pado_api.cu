@@ -210,10 +210,11 @@ bool grant_smem(StreamFn fn)
 // The streaming kernel's tiling for one (tables, direction, copy path).  The
 // candidates are tried in order of preference (16 lines and one stage, two
 // CTAs per SM, is fastest for every operator at n = 512; a larger tile only
-// pays for short x lines); the first that fits two CTAs per SM wins, else the
-// one with the most resident warps.  One exception, measured on x lines of
-// 64 to 256 points: 32 lines per tile beat 16 by 4-22% whenever they keep at
-// least as many threads resident (two CTAs or more per SM).
+// pays for short lines); the first that fits two CTAs per SM wins, else the
+// one with the most resident warps.  One exception, measured on lines of 64
+// to 256 points: 32 lines per tile beat 16 by 3-24% (x lines, and y/z lines
+// of every operator but bounded cd06, which keeps 16 from n = 256) whenever
+// they keep at least as many threads resident (two CTAs or more per SM).
 bool choose_stream_tiling(const pado_op_s *op, const DevTables &dt, const KParams &kp0, bool xl, bool as, bool adj,
                           int etab_rows, int ktab_rows, StreamChoice *out)
 {
@@ -231,7 +232,6 @@ bool choose_stream_tiling(const pado_op_s *op, const DevTables &dt, const KParam
         int nslots = warp_slots(dt.host, L, perm, KMAXSLOT, true);
         if (L * nslots > 384) nslots = warp_slots(dt.host, L, perm, KMAXSLOT, false);
         if (L * nslots > 384) continue;  // the kernel is built for 384 threads, two CTAs per SM
-        if (!xl && L == 32) continue;  // strided-line kernels exist for 8 and 16 lines per tile
         if (op->stream_lines && L != op->stream_lines) continue;
         if (op->stream_stages && stages != op->stream_stages) continue;
         StreamFn fn = pick_stream(kp0.rc.rk, op->periodic != 0, op->m, xl, L, adj, as);
@@ -256,7 +256,8 @@ bool choose_stream_tiling(const pado_op_s *op, const DevTables &dt, const KParam
     int pick = -1;
     for (int i = 0; i < 6 && pick < 0; ++i)
         if (res[i].ok && res[i].c.ctas >= 2) pick = i;
-    if (pick == 0 && xl && res[1].ok && res[1].c.ctas >= 2 && resident(1) >= resident(0)) pick = 1;
+    const bool keep16 = !xl && op->scheme == CD06 && !op->periodic && n >= 256;  // measured 5% faster at 16
+    if (pick == 0 && !keep16 && res[1].ok && res[1].c.ctas >= 2 && resident(1) >= resident(0)) pick = 1;
     if (pick < 0) {
         long long best = -1;
         for (int i = 0; i < 6; ++i)

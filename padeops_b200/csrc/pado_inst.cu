@@ -54,6 +54,7 @@ template <bool PER, bool ADJ, bool AS>
 StreamFn pick_stream_l(int m, bool xl, int lines)
 {
     if (xl) return pick_stream_m<PER, true, 0, ADJ, AS>(m);
+    if (lines == 32) return pick_stream_m<PER, false, 32, ADJ, AS>(m);
     return lines == 8 ? pick_stream_m<PER, false, 8, ADJ, AS>(m) : pick_stream_m<PER, false, 16, ADJ, AS>(m);
 }
 

@@ -86,7 +86,7 @@ KernelFn pick_kernel_rk1(bool per, bool adj, bool contiguous, int m, int variant
 KernelFn pick_kernel_rk2(bool per, bool adj, bool contiguous, int m, int variant);
 KernelFn pick_kernel_rk3(bool per, bool adj, bool contiguous, int m, int variant);
 using StreamFn = void (*)(const StreamParams);
-// streaming kernels: strided lines are built for 8 or 16 lines per tile
+// streaming kernels: strided lines are built for 8, 16 or 32 lines per tile
 // (`lines`), x lines for any; adj: the adjoint (transposed sweep, then B^T)
 StreamFn pick_stream_rk0(bool per, int m, bool xl, int lines, bool adj, bool as);
 StreamFn pick_stream_rk1(bool per, int m, bool xl, int lines, bool adj, bool as);
