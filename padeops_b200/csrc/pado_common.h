@@ -41,6 +41,17 @@ constexpr int HALO = 4;
 // the interior stencil).  cd06.F90:567-585, cd10.F90:1164-1258 / 1656-1730,
 // cf90.F90:676-798.
 PADO_HD PADO_INLINE int closure_rows(int rk) { return rk == RHS_CD06_D1 ? 3 : (rk == RHS_CD10_D2 ? 3 : 4); }
+// Rows of an edge piece (the rows outside the constant-coefficient block,
+// cut into pieces the kernels run fully unrolled) for segments of m rows:
+// m/4 for cd06 and the cd10 second derivative, m/2 for the others (measured
+// on 512^3: the shorter pieces give cd06 and cd10 d2 more resident threads
+// and run 2-6% faster; the cd10 first derivative and cf90 lose 1-40% with
+// them, cf90 because its longer edge region then needs more segments than
+// a 16-line tile of 384 threads holds).
+PADO_HD constexpr int edge_piece_rows(int rk, int m)
+{
+    return (rk == RHS_CD06_D1 || rk == RHS_CD10_D2) && m / 4 >= 5 ? m / 4 : m / 2;
+}
 
 // Stencil coefficients, already scaled by 1/dx or 1/dx^2 as the reference
 // scales them inside ComputeXD1RHS & co.

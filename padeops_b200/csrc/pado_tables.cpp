@@ -385,7 +385,7 @@ Sweep adjoint_sweep(const Sweep &p)
     return a;
 }
 
-Layout make_layout(int n, int m, int i0, int i1)
+Layout make_layout(int n, int m, int i0, int i1, int e_rows)
 {
     Layout L;
     L.n = n;
@@ -400,12 +400,12 @@ Layout make_layout(int n, int m, int i0, int i1)
         uniform((n + m - 1) / m);
         return L;
     }
-    // Lines whose length is a multiple of E = m/2: pieces of exactly E rows
-    // before and after the interior block, which the kernels run on a fully
-    // unrolled per-row-table path (about as fast per row as the interior);
-    // the block of k interior segments starts at a whole number of pieces
-    // (one interior segment fewer where the rounding needs it).
-    const int E = m / 2;
+    // Lines whose length is a multiple of E (e_rows, else m/2): pieces of
+    // exactly E rows before and after the interior block, which the kernels
+    // run on a fully unrolled per-row-table path (about as fast per row as
+    // the interior); the block of k interior segments starts at a whole
+    // number of pieces (one interior segment fewer where the rounding needs it).
+    const int E = e_rows > 0 ? e_rows : m / 2;
     if (n % E == 0) {
         const int A = (A0 + E - 1) / E * E;
         for (int k = kmax; k >= std::max(1, kmax - 1); --k) {
@@ -718,7 +718,7 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     ot.rc = make_rhs_coef(scheme, kind, dx, periodic);
     int i0, i1;
     interior_range(sw, &i0, &i1);
-    ot.lay = make_layout(n, m, i0, i1);
+    ot.lay = make_layout(n, m, i0, i1, edge_piece_rows(ot.rc.rk, m));
     std::vector<double> segsum;
     build_device_table(sw, ot.lay, ot.tab, segsum);
     ot.interior = interior_info(sw, ot.lay, m);
@@ -779,7 +779,7 @@ int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots, b
     // and border responses
     auto cls = [&](int s) {
         const int a = ot.lay.start(s), len = ot.lay.len(s);
-        if (!((ot.interior.mask >> s) & 1u)) return len == ot.m / 2 ? 0 : 1;
+        if (!((ot.interior.mask >> s) & 1u)) return len == edge_piece_rows(ot.rc.rk, ot.m) ? 0 : 1;
         const bool spk = (ot.interior.spk_mask >> s) & 1u;
         const bool resp = ot.nbord > 0 && (a < ot.ie || a + len > ot.je);
         return spk ? (resp ? 2 : 3) : (resp ? 4 : 5);

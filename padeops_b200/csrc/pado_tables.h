@@ -42,12 +42,13 @@ struct Layout {
     int len(int s) const { return st[s + 1] - st[s]; }
 };
 // With an interior [i0, i1) (i0 < i1): as many segments of exactly m rows as
-// fit in it, and the rows before and after cut into pieces of m/2 rows (the
-// kernels' fully unrolled per-row-table path) when n is a multiple of m/2,
-// else into near-equal pieces of about m/3 rows (the generic per-row loop).
+// fit in it, and the rows before and after cut into pieces of e_rows rows
+// (edge_piece_rows of pado_common.h; 0: m/2), the kernels' fully unrolled
+// per-row-table path, when n is a multiple of e_rows, else into near-equal
+// pieces of about m/3 rows (the generic per-row loop).
 // Without one: ceil(n/m) segments of near-equal length.
 constexpr int MAX_SEGMENTS = 32;
-Layout make_layout(int n, int m, int i0 = 0, int i1 = 0);
+Layout make_layout(int n, int m, int i0 = 0, int i1 = 0, int e_rows = 0);
 // Banded rows [i0, i1) whose coefficients have settled (see Interior);
 // i0 == i1 == 0 when there are none.
 void interior_range(const Sweep &sw, int *i0, int *i1);
