@@ -43,14 +43,16 @@ constexpr int HALO = 4;
 PADO_HD PADO_INLINE int closure_rows(int rk) { return rk == RHS_CD06_D1 ? 3 : (rk == RHS_CD10_D2 ? 3 : 4); }
 // Rows of an edge piece (the rows outside the constant-coefficient block,
 // cut into pieces the kernels run fully unrolled) for segments of m rows:
-// m/4 for cd06 and the cd10 second derivative, m/2 for the others (measured
-// on 512^3: the shorter pieces give cd06 and cd10 d2 more resident threads
-// and run 2-6% faster; the cd10 first derivative and cf90 lose 1-40% with
-// them, cf90 because its longer edge region then needs more segments than
-// a 16-line tile of 384 threads holds).
-PADO_HD constexpr int edge_piece_rows(int rk, int m)
+// m/4 for cd06 and the cd10 second derivative, m for the bounded cf90, m/2
+// for the others.  Measured on 512^3: the shorter pieces give cd06 and cd10
+// d2 more resident threads and run 2-6% faster; the cd10 first derivative
+// and cf90 lose 1-40% with them (cf90's longer edge region then needs more
+// segments than a 16-line tile of 384 threads holds); pieces of m rows make
+// the bounded cf90 4-10% faster and the periodic one 7-10% slower.
+PADO_HD constexpr int edge_piece_rows(int rk, bool periodic, int m)
 {
-    return (rk == RHS_CD06_D1 || rk == RHS_CD10_D2) && m / 4 >= 5 ? m / 4 : m / 2;
+    return (rk == RHS_CD06_D1 || rk == RHS_CD10_D2) && m / 4 >= 5 ? m / 4
+                                                                   : (rk == RHS_CF90 && !periodic ? m : m / 2);
 }
 
 // Stencil coefficients, already scaled by 1/dx or 1/dx^2 as the reference

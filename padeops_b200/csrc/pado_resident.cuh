@@ -176,7 +176,7 @@ struct ResidentLine {
     // outside the constant-coefficient block into such pieces): the per-row
     // table path fully unrolled, every tile and table offset an immediate, no
     // per-row bounds; the same arithmetic as the generic per-row loop.
-    static constexpr int E = edge_piece_rows(RK, M);
+    static constexpr int E = edge_piece_rows(RK, PER, M);
     static_assert(E >= 5, "the unrolled edge path needs pieces of at least 5 rows");
 
     // the same address, marked for the compiler as shared memory (tile and

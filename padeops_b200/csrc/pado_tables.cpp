@@ -718,7 +718,7 @@ OpTables make_op_tables(int scheme, int kind, int n, double dx, int periodic, in
     ot.rc = make_rhs_coef(scheme, kind, dx, periodic);
     int i0, i1;
     interior_range(sw, &i0, &i1);
-    ot.lay = make_layout(n, m, i0, i1, edge_piece_rows(ot.rc.rk, m));
+    ot.lay = make_layout(n, m, i0, i1, edge_piece_rows(ot.rc.rk, ot.rc.periodic != 0, m));
     std::vector<double> segsum;
     build_device_table(sw, ot.lay, ot.tab, segsum);
     ot.interior = interior_info(sw, ot.lay, m);
@@ -779,7 +779,7 @@ int warp_slots(const OpTables &ot, int L, unsigned char *sperm, int max_slots, b
     // and border responses
     auto cls = [&](int s) {
         const int a = ot.lay.start(s), len = ot.lay.len(s);
-        if (!((ot.interior.mask >> s) & 1u)) return len == edge_piece_rows(ot.rc.rk, ot.m) ? 0 : 1;
+        if (!((ot.interior.mask >> s) & 1u)) return len == edge_piece_rows(ot.rc.rk, ot.rc.periodic != 0, ot.m) ? 0 : 1;
         const bool spk = (ot.interior.spk_mask >> s) & 1u;
         const bool resp = ot.nbord > 0 && (a < ot.ie || a + len > ot.je);
         return spk ? (resp ? 2 : 3) : (resp ? 4 : 5);
