@@ -48,7 +48,7 @@ def _rel(x, r):
 @pytest.mark.parametrize("periodic", [True, False])
 def test_stream_kernel_emulated(emul, scheme, kind, periodic):
     rng = np.random.default_rng(3 + scheme + 5 * kind)
-    for n, m, lines in [(10, 32, 16), (34, 16, 8), (100, 32, 16), (256, 32, 16), (320, 64, 8)]:
+    for n, m, lines in [(10, 32, 16), (34, 16, 8), (100, 32, 16), (256, 32, 16), (320, 64, 8), (512, 32, 16)]:
         for bc1, bcn in _bcs(scheme, periodic):
             dx = 0.37
             op = oracle.OracleOp(scheme, n, dx, periodic, bc1, bcn)
