@@ -162,9 +162,14 @@ def _z_to_y_send(s: Slabs, fz: torch.Tensor) -> tuple[torch.Tensor, list[int], l
     nz, n2, n1 = s.z_shape()
     if tuple(fz.shape) != (nz, n2, n1) or not fz.is_contiguous():
         raise ValueError(f"expected this rank's contiguous z-slab of shape {(nz, n2, n1)}")
-    chunks = [fz[:, y0:y1, :].reshape(-1) for y0, y1 in (s.y_range(r) for r in range(s.size))]
-    send = torch.cat(chunks) if chunks else fz.reshape(-1)
-    send_counts = [c.numel() for c in chunks]
+    send = torch.empty(fz.numel(), dtype=fz.dtype, device=fz.device)
+    send_counts, off = [], 0
+    for r in range(s.size):  # the y chunk for rank r, packed by one copy
+        y0, y1 = s.y_range(r)
+        cnt = nz * (y1 - y0) * n1
+        send[off:off + cnt].view(nz, y1 - y0, n1).copy_(fz[:, y0:y1, :])
+        send_counts.append(cnt)
+        off += cnt
     ny = s.y_shape()[1]
     recv_counts = [s.z_shape(r)[0] * ny * n1 for r in range(s.size)]
     return send, send_counts, recv_counts
