@@ -6,9 +6,9 @@
 // resident in shared memory while
 // the tile-resident sweep of the streaming kernel (pado_resident.cuh) runs on
 // it.  Tiles of all items are numbered, most expensive item first; CTAs claim
-// tiles from a device counter (atomicAdd, no waiting on other CTAs) until the
-// list is exhausted.  A CTA claims its next tile while it solves the current
-// one, and as soon as the current tile's buffer is free every thread issues
+// tiles from a device counter, BATCH_CLAIM consecutive tiles at a time
+// (atomicAdd, no waiting on other CTAs), until the list is exhausted.  A CTA
+// claims its next tiles while it solves the current one, and as soon as the current tile's buffer is free every thread issues
 // 8-byte asynchronous copies (cp.async) of its share of the next tile, which
 // land on an mbarrier (one arrival per thread) while the other CTA on the SM
 // computes; the wait on it is bounded.  Results leave straight from the sweep
