@@ -164,3 +164,18 @@ extern "C" int emul_stencil(int scheme, int kind, int n, double dx, int periodic
     std::memcpy(B, b.data(), sizeof(double) * b.size());
     return 0;
 }
+
+// The segment layout and code-path facts of one operator's tables:
+// starts[0..S] (S = *nseg), fast[s] (constant-coefficient interior segment),
+// *edge (the unrolled edge-piece length), *w (coupling window).
+extern "C" int emul_layout(int scheme, int kind, int n, int periodic, int bc1, int bcn, int m, int *starts, int *fast,
+                           int *nseg, int *edge, int *w)
+{
+    const OpTables ot = make_op_tables(scheme, kind, n, 0.1, periodic, bc1, bcn, m, false);
+    *nseg = ot.lay.S;
+    for (int s = 0; s <= ot.lay.S; ++s) starts[s] = ot.lay.st[s];
+    for (int s = 0; s < ot.lay.S; ++s) fast[s] = (int)((ot.interior.mask >> s) & 1u);
+    *edge = edge_piece_rows(ot.rc.rk, periodic != 0, m);
+    *w = ot.chain.W;
+    return 0;
+}
