@@ -463,30 +463,53 @@ def run_gpu(args) -> None:
     if rank == 0 or world > 1:
         from padeops_b200.field_ops import apply_host_terms
 
-        hf = torch.from_numpy(f_host).pin_memory()
-        houts = [torch.empty_like(hf).pin_memory() for _ in plan]
-        terms = [(op, kind, axis, 0, 0, 1.0, 0.0, i) for i, (op, kind, axis) in enumerate(plan)]
+        field_bytes = N ** 3 * 8
         e2e_steps = max(1, min(args.steps, 3))
-        apply_host_terms(hf, (N, N, N), terms, houts)
+        hf = torch.from_numpy(f_host).pin_memory()
+        # nine pinned result buffers per rank (all ranks of a node pin theirs
+        # at once): only when they fit in half the host's available memory,
+        # else the per-operator host call alone, with one result buffer
+        try:
+            import psutil
+
+            avail = psutil.virtual_memory().available
+        except Exception:  # noqa: BLE001 -- no psutil: assume room for one rank's buffers
+            avail = 4 * len(plan) * field_bytes
+        local = int(os.environ.get("LOCAL_WORLD_SIZE", world))
+        terms_path = len(plan) * field_bytes * local <= avail // 2
+        hdf = torch.empty_like(hf).pin_memory()
+
+        def per_operator():
+            for op, kind, axis in plan:
+                op.apply_host(kind, axis, hf, hdf, N, N)
+
+        per_operator()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            apply_host_terms(hf, (N, N, N), terms, houts)
-        torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        hdf = houts[0]
         t1 = time.perf_counter()
-        for op, kind, axis in plan:
-            op.apply_host(kind, axis, hf, hdf, N, N)
+        for _ in range(e2e_steps):
+            per_operator()
         torch.cuda.synchronize()
-        el_op = time.perf_counter() - t1
-        e2e = {"value": 9 * N ** 3 * e2e_steps / el / 1e9 * world, "unit": "Gpts/s",
-               "h2d_bytes_per_step": N ** 3 * 8, "d2h_bytes_per_step": 9 * N ** 3 * 8,
-               "path": "pado_apply_host_terms: one upload of f, nine results downloaded (pinned host buffers)",
-               "per_operator_host_calls": {"value": round(9 * N ** 3 / el_op / 1e9, 3), "unit": "Gpts/s",
-                                           "h2d_bytes_per_step": 9 * N ** 3 * 8, "d2h_bytes_per_step": 9 * N ** 3 * 8,
-                                           "path": "pado_apply_host per operator"}}
-        del houts
+        el_op = (time.perf_counter() - t1) / e2e_steps
+        per_op = {"value": round(9 * N ** 3 / el_op / 1e9 * world, 3), "unit": "Gpts/s",
+                  "h2d_bytes_per_step": 9 * field_bytes, "d2h_bytes_per_step": 9 * field_bytes,
+                  "path": "pado_apply_host per operator (pinned host buffers)"}
+        if terms_path:
+            houts = [hdf] + [torch.empty_like(hf).pin_memory() for _ in plan[1:]]
+            terms = [(op, kind, axis, 0, 0, 1.0, 0.0, i) for i, (op, kind, axis) in enumerate(plan)]
+            apply_host_terms(hf, (N, N, N), terms, houts)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                apply_host_terms(hf, (N, N, N), terms, houts)
+            torch.cuda.synchronize()
+            el = (time.perf_counter() - t0) / e2e_steps
+            e2e = {"value": 9 * N ** 3 / el / 1e9 * world, "unit": "Gpts/s",
+                   "h2d_bytes_per_step": field_bytes, "d2h_bytes_per_step": 9 * field_bytes,
+                   "path": "pado_apply_host_terms: one upload of f, nine results downloaded (pinned host buffers)",
+                   "per_operator_host_calls": per_op}
+            del houts
+        else:
+            e2e = dict(per_op)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
