@@ -288,12 +288,11 @@ bool plan_stream(const pado_op_s *op, const DevTables &dt, const KParams &kp0, i
     // Some x lines run faster from the odd-pitch tile the per-element copies
     // fill (no bank conflicts between the lines a warp sweeps) than from the
     // bulk copies' even pitch.  Measured (B200, lines of 128 to 1024 points):
-    // cd06 for n = 128..512 (4-17% faster), bounded cd10 d1 and cf90 for
-    // n = 256..512 (2-9%); every other case, and every n = 1024, is 3-19%
-    // slower with them and keeps the bulk copies.
-    const bool bounded10 = !op->periodic && op->scheme != CD06 && kp0.rc.rk != RHS_CD10_D2;
-    const bool prefer_async =
-        xl && !adj && ((op->scheme == CD06 && n >= 128 && n <= 512) || (bounded10 && n >= 256 && n <= 512));
+    // cd06 and the bounded operators for n = 128..512 (2-17% faster; the
+    // bounded cd10 d2 only from n = 256); the periodic cd10 and cf90, and
+    // every n = 1024, are 0-20% slower with them and keep the bulk copies.
+    const bool prefer_async = xl && !adj && n >= 128 && n <= 512 &&
+                              (op->scheme == CD06 || (!op->periodic && (kp0.rc.rk != RHS_CD10_D2 || n >= 256)));
     const bool as_ok = !adj && !(align_bits & 7);
     bool as = op->variant == 6 || (op->variant == 0 && (!tma_ok || prefer_async));
     if (as && !as_ok && op->variant == 0 && tma_ok) as = false;

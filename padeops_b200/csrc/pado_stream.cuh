@@ -26,8 +26,10 @@
 // mbarrier when they land (cp.async.mbarrier.arrive.noinc, one arrival per
 // thread), so the copies still run while the other CTAs on the SM compute.
 // x-line tiles then use an odd pitch P (no bank conflicts between lines)
-// and go back to global memory by coalesced stores from all threads.  The per-row table of the segments that read it and the
-// chain coefficients are staged in shared memory once per CTA.  Every wait
+// and go back to global memory by coalesced stores from all threads.
+//
+// The per-row table of the segments that read it and the chain
+// coefficients are staged in shared memory once per CTA.  Every wait
 // is bounded (2 s); on expiry the CTA records PADO_E_TIMEOUT in *status,
 // waits (bounded) for its copies in flight and returns.
 #pragma once
